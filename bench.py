@@ -1,0 +1,568 @@
+#!/usr/bin/env python
+"""Benchmark of the CSR SpMV / SpMM hot path on B200.
+
+Default workload (one step = one SpMM over one batch of synthetic input):
+power-law CSR SpMM, 262144 x 262144, Zipf(1.8) row lengths scaled to mean ~12
+and capped at 20000, uniform columns, U(-1,1) float32 values, int32 indices,
+dense B 262144 x 64 float32 N(0,1), C 262144 x 64 float32.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+Prints one JSON line (rank 0).  ``value`` is the useful HBM bytes per second
+of the chosen form (launch plan from the selector / heuristic, float32
+accumulation), summed over all ranks, with inputs resident in HBM and L2
+flushed (256 MiB write) before every timed step; ``plain`` reports the
+FlagSparse-compatible plain form (float64 accumulation) the same way; ``e2e``
+runs the public API from pinned host buffers (host->device copies of A and B,
+prepare, SpMM, device->host copy of C) every step.  ``--impl reference`` times
+the CPU restatement of FlagSparse's algorithm (the oracle port) on the host
+cores instead.
+
+Multi-GPU: one process per GPU (torchrun), each rank runs the same workload
+on its own GPU (replicas; the path needs no data exchange), timed on the
+device, max over ranks.
+"""
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+L2_FLUSH_BYTES = 256 << 20
+FALLBACK_HBM_GBS = 6650.0
+
+
+# ----------------------------------------------------------------- setup ----
+def parse_args(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=50)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--workload", default="spmm_powerlaw", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-e2e", action="store_true", help="skip the end-to-end leg")
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--profile", action="store_true",
+                    help="only warm-up + timed device steps (for a profiler launch list)")
+    return ap.parse_args(argv)
+
+
+def dist_env():
+    return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
+
+
+def init_dist(world):
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+
+
+def max_over_ranks(value, world):
+    if world == 1:
+        return value
+    import torch.distributed as dist
+
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def measured_peak_hbm():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def committed_traffic(kernel_key):
+    """DRAM bytes per launch from a committed ncu summary (profiles/*.txt)."""
+    path = os.path.join(ROOT, "profiles", f"{kernel_key}.txt")
+    try:
+        for line in open(path):
+            if line.startswith("dram_bytes_per_launch:"):
+                return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        pass
+    return None
+
+
+# ---------------------------------------------------------- clock sampling --
+class ClockSampler:
+    """Samples SM clocks and clock-event reasons of one GPU through NVML."""
+
+    REASONS = {
+        "hw_slowdown": 0x8,
+        "sw_thermal_slowdown": 0x20,
+        "hw_thermal_slowdown": 0x40,
+        "hw_power_brake_slowdown": 0x80,
+        "sw_power_cap": 0x4,
+    }
+
+    def __init__(self, device_index, period_s=0.01):
+        self.samples = []
+        self.max_mhz = None
+        self.ok = False
+        self.period = period_s
+        self._stop = threading.Event()
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            uuid = str(torch.cuda.get_device_properties(device_index).uuid)
+            if not uuid.startswith("GPU-"):
+                uuid = "GPU-" + uuid
+            self.h = pynvml.nvmlDeviceGetHandleByUUID(uuid)
+            self.nvml = pynvml
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:  # noqa: BLE001 -- clocks are reported as unavailable
+            self.ok = False
+
+    def _run(self):
+        nv = self.nvml
+        while not self._stop.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                reasons = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.samples.append((sm, reasons))
+            except Exception:  # noqa: BLE001
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok or not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": self.max_mhz, "reasons": [], "samples": 0}
+        sms = [s for s, _ in self.samples]
+        active = set()
+        for _, r in self.samples:
+            for name, bit in self.REASONS.items():
+                if r & bit:
+                    active.add(name)
+        return {"sm_mhz": float(statistics.median(sms)), "sm_max_mhz": self.max_mhz, "reasons": sorted(active),
+                "samples": len(sms)}
+
+
+# --------------------------------------------------------------- workloads --
+class SpmmPowerlaw:
+    """Power-law CSR SpMM (262144^2, Zipf 1.8, mean ~12, cap 20000, N = 64, fp32)."""
+
+    metric = "CSR SpMM useful HBM throughput (chosen form)"
+    unit = "GB/s"
+
+    def __init__(self, n_rows=262144, n_dense=64, seed=0):
+        self.n_rows = n_rows
+        self.n_dense = n_dense
+        self.seed = seed
+
+    def generate(self, device):
+        """Seeded inputs only (no kernel of this project runs here)."""
+        from flagsparse_public_b200 import synthetic
+
+        data, indices, indptr, shape = synthetic.zipf_powerlaw(self.n_rows, self.n_rows, alpha=1.8, mean=12.0,
+                                                               cap=20000, seed=self.seed, dtype=torch.float32,
+                                                               device=device)
+        B = synthetic.dense_operand(shape[1], self.n_dense, seed=self.seed + 1, dtype=torch.float32, device=device)
+        self.A = (data, indices, indptr)
+        self.shape = shape
+        self.B = B
+        self.nnz = data.numel()
+        self.useful_bytes = self.nnz * (4 + 4) + shape[1] * self.n_dense * 4 + shape[0] * self.n_dense * 4
+        self.flops = 2 * self.nnz * self.n_dense
+        lens = (indptr[1:] - indptr[:-1])
+        self.row_stats = {"mean_row": float(lens.float().mean()), "max_row": int(lens.max())}
+
+    def build(self, device):
+        import flagsparse_public_b200 as fs
+
+        self.generate(device)
+        data, indices, indptr = self.A
+        self.C = torch.empty((self.shape[0], self.n_dense), dtype=torch.float32, device=device)
+        self.prepared = fs.prepare_spmm_csr_opt(data, indices, indptr, self.shape)
+
+    def config(self):
+        return {
+            "workload": f"csr_spmm_powerlaw_{self.shape[0]}x{self.shape[1]}_zipf1.8_mean12_cap20000_n{self.n_dense}"
+                        "_f32_i32",
+            "n_rows": self.shape[0], "n_cols": self.shape[1], "nnz": self.nnz, "n_dense": self.n_dense,
+            "global_batch": 1, "useful_bytes_per_step": self.useful_bytes, **self.row_stats,
+            "l2": "flushed before every timed step (256 MiB write)",
+            "parallelism": "replicas",
+        }
+
+    def step(self):
+        import flagsparse_public_b200 as fs
+
+        fs.flagsparse_spmm_csr_opt(B=self.B, prepared=self.prepared, out=self.C)
+
+    def plain_step(self):
+        import flagsparse_public_b200.sparse_operations.spmm_csr as mm
+
+        data, indices, indptr = self.A
+        if not hasattr(self, "_alg1_plan"):
+            holder = mm._Alg1Holder(data, indptr, self.shape[0], self.shape[1], self.row_stats["max_row"], self.nnz)
+            self._alg1_plan = mm._spmm_plan_for(holder, "alg1", self.n_dense)
+        mm._triton_spmm_csr_impl(data, indices, indptr, self.B, self.shape[0], self.n_dense, 0, 0,
+                                 out=self.C, plan=self._alg1_plan)
+
+    def plan_desc(self):
+        from flagsparse_public_b200.sparse_operations.spmm_csr import _spmm_plan_for
+
+        return _spmm_plan_for(self.prepared, "opt", self.n_dense).describe()
+
+    # end to end through the public API from pinned host memory
+    def host_inputs(self):
+        data, indices, indptr = self.A
+        self.h = [t.cpu().pin_memory() for t in (data, indices, indptr, self.B)]
+        self.h_out = torch.empty(self.C.shape, dtype=self.C.dtype).pin_memory()
+        self.h2d_bytes = sum(t.numel() * t.element_size() for t in self.h)
+        self.d2h_bytes = self.h_out.numel() * self.h_out.element_size()
+
+    def e2e_step(self, device):
+        import flagsparse_public_b200 as fs
+
+        d = [t.to(device, non_blocking=True) for t in self.h]
+        C = fs.flagsparse_spmm_csr_opt(d[0], d[1], d[2], d[3], self.shape)
+        self.h_out.copy_(C, non_blocking=True)
+
+    def fp64_error(self):
+        """Condition-scaled error of chosen and plain results vs the FP64 oracle."""
+        from oracle import oracle as orc
+        from tests.numerics import scaled_error
+
+        data, indices, indptr = (t.cpu() for t in self.A)
+        exact, mag = orc.spmm_csr_exact(data, indices, indptr, self.B.cpu())
+        self.step()
+        chosen = scaled_error(self.C.cpu(), exact, mag)
+        self.plain_step()
+        plain = scaled_error(self.C.cpu(), exact, mag)
+        return {"chosen": chosen, "plain": plain, "definition": "max |c - c64| / sum_k |a_k b_k|"}
+
+    def cpu_step_factory(self, threads, sample_rows=None):
+        """Oracle port of FlagSparse's plain SpMM (float64 accumulation) on host cores."""
+        from oracle import oracle as orc
+
+        data, indices, indptr = (t.cpu() for t in self.A)
+        B = self.B.cpu()
+        rows = self.shape[0] if sample_rows is None else min(sample_rows, self.shape[0])
+        sub_ptr = indptr[: rows + 1].clone()
+        k = int(sub_ptr[-1])
+        sub = (data[:k], indices[:k], sub_ptr)
+        frac_bytes = k * 8 + self.shape[1] * self.n_dense * 4 + rows * self.n_dense * 4
+
+        def run():
+            orc.spmm_csr(sub[0], sub[1], sub[2], B, acc_mode=orc.ACC_WIDE, threads=threads)
+
+        return run, frac_bytes, f"rows [0, {rows}) of the workload ({k} nonzeros), N = {self.n_dense}"
+
+
+class SpmvPoisson:
+    """CSR SpMV 16384^2, Poisson(16) rows, fp32 -- L2-resident, timed as a CUDA
+    graph of 1000 back-to-back launches per step."""
+
+    metric = "CSR SpMV useful throughput (L2-resident, graph of 1000 launches)"
+    unit = "GB/s"
+    graph_iters = 1000
+
+    def generate(self, device):
+        from flagsparse_public_b200 import synthetic
+
+        data, indices, indptr, shape = synthetic.poisson_uniform(seed=0, device=device)
+        self.A = (data, indices, indptr)
+        self.shape = shape
+        self.x = synthetic.dense_vector(shape[1], seed=1, device=device)
+        self.nnz = data.numel()
+        self.useful_bytes = (self.nnz * 8 + shape[1] * 4 + shape[0] * 4) * self.graph_iters
+        self.flops = 2 * self.nnz * self.graph_iters
+
+    def build(self, device):
+        import flagsparse_public_b200 as fs
+
+        self.generate(device)
+        data, indices, indptr = self.A
+        self.y = torch.empty(self.shape[0], device=device)
+        self.prepared = fs.prepare_spmv_csr(data, indices, indptr, self.shape)
+        fs.flagsparse_spmv_csr(x=self.x, prepared=self.prepared, out=self.y, use_opt=True)
+        fs.flagsparse_spmv_csr(x=self.x, prepared=self.prepared, out=self.y, use_opt=False)
+        self.graph = self._capture(use_opt=True)
+        self.graph_plain = self._capture(use_opt=False)
+
+    def _capture(self, use_opt):
+        import flagsparse_public_b200 as fs
+
+        g = torch.cuda.CUDAGraph()
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(s):
+            for _ in range(3):
+                fs.flagsparse_spmv_csr(x=self.x, prepared=self.prepared, out=self.y, use_opt=use_opt)
+        torch.cuda.current_stream().wait_stream(s)
+        with torch.cuda.graph(g):
+            for _ in range(self.graph_iters):
+                fs.flagsparse_spmv_csr(x=self.x, prepared=self.prepared, out=self.y, use_opt=use_opt)
+        return g
+
+    def config(self):
+        return {"workload": "csr_spmv_poisson16_16384x16384_f32_i32_graph1000", "n_rows": self.shape[0],
+                "nnz": self.nnz, "global_batch": self.graph_iters,
+                "l2": "L2-resident by design (2.2 MB working set)", "parallelism": "replicas"}
+
+    def step(self):
+        self.graph.replay()
+
+    def plain_step(self):
+        self.graph_plain.replay()
+
+    def plan_desc(self):
+        from flagsparse_public_b200.sparse_operations.spmv_csr import _spmv_plan
+
+        return _spmv_plan(self.prepared, "opt").describe()
+
+    def host_inputs(self):
+        data, indices, indptr = self.A
+        self.h = [t.cpu().pin_memory() for t in (data, indices, indptr, self.x)]
+        self.h_out = torch.empty(self.y.shape, dtype=self.y.dtype).pin_memory()
+        self.h2d_bytes = sum(t.numel() * t.element_size() for t in self.h)
+        self.d2h_bytes = self.h_out.numel() * self.h_out.element_size()
+
+    def e2e_step(self, device):
+        import flagsparse_public_b200 as fs
+
+        d = [t.to(device, non_blocking=True) for t in self.h]
+        y = fs.flagsparse_spmv_csr(d[0], d[1], d[2], d[3], self.shape, use_opt=True)
+        self.h_out.copy_(y, non_blocking=True)
+
+    def fp64_error(self):
+        from oracle import oracle as orc
+        from tests.numerics import scaled_error
+        import flagsparse_public_b200 as fs
+
+        data, indices, indptr = (t.cpu() for t in self.A)
+        exact, mag = orc.spmv_csr_exact(data, indices, indptr, self.x.cpu())
+        y1 = fs.flagsparse_spmv_csr(x=self.x, prepared=self.prepared, use_opt=True)
+        y2 = fs.flagsparse_spmv_csr(x=self.x, prepared=self.prepared, use_opt=False)
+        return {"chosen": scaled_error(y1, exact, mag), "plain": scaled_error(y2, exact, mag),
+                "definition": "max |y - y64| / sum_k |a_k x_k|"}
+
+    def cpu_step_factory(self, threads, sample_rows=None):
+        from oracle import oracle as orc
+
+        data, indices, indptr = (t.cpu() for t in self.A)
+        x = self.x.cpu()
+        per_call = self.nnz * 8 + self.shape[1] * 4 + self.shape[0] * 4
+
+        def run():
+            for _ in range(100):
+                orc.spmv_csr(data, indices, indptr, x, acc_mode=orc.ACC_WIDE, threads=threads)
+
+        return run, per_call * 100, "100 calls of the full SpMV"
+
+
+WORKLOADS = {"spmm_powerlaw": SpmmPowerlaw, "spmv_poisson": SpmvPoisson}
+
+
+# ------------------------------------------------------------------ timing --
+def time_device_steps(fn, steps, flush):
+    """CUDA-event time of each step on the current stream, L2 flushed before each."""
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for i in range(steps):
+        if flush is not None:
+            flush.zero_()
+        starts[i].record()
+        fn()
+        ends[i].record()
+    torch.cuda.synchronize()
+    return [s.elapsed_time(e) for s, e in zip(starts, ends)]
+
+
+def time_cpu(run, min_seconds=10.0, max_seconds=30.0, min_reps=3):
+    run()  # warm-up
+    times = []
+    t_end = time.perf_counter() + min_seconds
+    while (len(times) < min_reps or time.perf_counter() < t_end) and sum(times) < max_seconds:
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    return statistics.median(times), len(times)
+
+
+def cpu_threads():
+    try:
+        return len(os.sched_getaffinity(0))
+    except AttributeError:
+        return os.cpu_count() or 1
+
+
+# -------------------------------------------------------------------- arms --
+def run_reference(args):
+    """FlagSparse's algorithm restated for the CPU (oracle port), host cores."""
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return 0
+    wl = WORKLOADS[args.workload]()
+    dev = "cuda" if torch.cuda.is_available() else "cpu"
+    wl.generate(dev)
+    threads = cpu_threads()
+    run, nbytes, sample = wl.cpu_step_factory(threads)
+    for _ in range(max(args.warmup, 1)):
+        run()
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        run()
+        times.append(time.perf_counter() - t0)
+    ms = 1000.0 * statistics.mean(times)
+    value = nbytes / (ms * 1e-3) / 1e9
+    line = {
+        "impl": "reference", "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": wl.config(),
+        "cpu_baseline": {"value": value, "unit": wl.unit, "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": wl.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    from flagsparse_public_b200 import _plan
+
+    rank, world, local_rank = dist_env()
+    init_dist(world)
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    wl = WORKLOADS[args.workload]()
+    wl.build(device)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+
+    for _ in range(args.warmup):
+        wl.step()
+    torch.cuda.synchronize()
+    barrier(world)
+    launches0 = _plan.LAUNCHES["count"]
+    with ClockSampler(local_rank) as clocks:
+        times = time_device_steps(wl.step, args.steps, flush)
+    graph_launches = getattr(wl, "graph_iters", 0)
+    launches = _plan.LAUNCHES["count"] - launches0
+    if graph_launches:
+        # graph replays launch the captured kernels without passing through Python
+        launches = args.steps * graph_launches * (2 if wl.plan_desc()["kind"] == "merge_path" else 1)
+    barrier(world)
+    total_ms = max_over_ranks(sum(times), world)
+    ms_step = total_ms / args.steps
+    value = wl.useful_bytes * world / (ms_step * 1e-3) / 1e9
+    if args.profile:
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "ms_per_step": ms_step}), flush=True)
+        return 0
+
+    # plain (FlagSparse-compatible) form, same protocol
+    for _ in range(args.warmup):
+        wl.plain_step()
+    torch.cuda.synchronize()
+    plain_times = time_device_steps(wl.plain_step, args.steps, flush)
+    plain_ms = max_over_ranks(sum(plain_times), world) / args.steps
+    plain_value = wl.useful_bytes * world / (plain_ms * 1e-3) / 1e9
+
+    e2e = None
+    if not args.no_e2e:
+        wl.host_inputs()
+        for _ in range(max(1, min(args.warmup, 3))):
+            wl.e2e_step(device)
+        torch.cuda.synchronize()
+        barrier(world)
+        e_steps = max(3, min(args.steps, 20))
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(e_steps):
+            wl.e2e_step(device)
+        e.record()
+        torch.cuda.synchronize()
+        e_ms = max_over_ranks(s.elapsed_time(e), world) / e_steps
+        per_step_bytes = wl.useful_bytes / getattr(wl, "graph_iters", 1)
+        e2e = {"value": per_step_bytes * world / (e_ms * 1e-3) / 1e9, "unit": wl.unit, "ms_per_step": e_ms,
+               "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes,
+               "what": "pinned host A and dense operand -> device, public one-shot API (prepare + product), "
+                       "result -> pinned host"}
+
+    errors = wl.fp64_error() if rank == 0 else None
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        threads = cpu_threads()
+        run, nbytes, sample = wl.cpu_step_factory(threads)
+        sec, reps = time_cpu(run)
+        cpu = {"value": nbytes / sec / 1e9, "unit": wl.unit, "cores": threads, "kind": "port",
+               "sample": f"{sample}; median of {reps} runs", "ms": sec * 1e3}
+
+    peak, peak_kind = measured_peak_hbm()
+    achieved = wl.useful_bytes / (statistics.mean(times) * 1e-3) / 1e9
+    kernel_key = f"traffic_{args.workload}"
+    traffic = committed_traffic(kernel_key)
+    if rank == 0:
+        line = {
+            "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, no dataset)",
+            "config": {**wl.config(), "plan": wl.plan_desc()},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
+                         "what": "useful bytes / mean CUDA-event duration of one product call"},
+            "plain": {"value": plain_value, "unit": wl.unit, "ms_per_step": plain_ms,
+                      "frac": plain_value / world / peak, "accumulation": "float64 (FlagSparse plain)"},
+            "error_vs_fp64": errors,
+            "e2e": e2e,
+            "cpu_baseline": cpu,
+            "gpu_launches": launches,
+            "clocks": clocks.summary(),
+            "gflops": wl.flops * world / (ms_step * 1e-3) / 1e9,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+    return 0
+
+
+def main(argv=None):
+    args = parse_args(argv)
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,196 @@
+"""ctypes binding of ``libflagsparse_b200.so`` (the C ABI in include/flagsparse_b200.h).
+
+Every compute entry point receives device pointers taken from torch tensors and
+the handle of torch's current CUDA stream; torch only provides memory and the
+stream.  There is no fallback: if the library is missing or a launch fails the
+caller gets an exception.
+"""
+
+import ctypes
+import os
+import threading
+
+import torch
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libflagsparse_b200.so")
+
+FSB_OK = 0
+FSB_ERR_INVALID = -1
+FSB_ERR_UNSUPPORTED = -2
+FSB_ERR_LAUNCH = -3
+FSB_ERR_WORKSPACE = -4
+FSB_ERR_TIMEOUT = -5
+FSB_ERR_LIMIT = -6
+
+FSB_F16, FSB_BF16, FSB_F32, FSB_F64, FSB_C64, FSB_C128, FSB_I32, FSB_I64 = range(8)
+ACC_NATIVE, ACC_WIDE, ACC_COMP = 0, 1, 2
+ALGO_ROWS, ALGO_MERGE = 0, 1
+
+_DTYPE_CODES = {
+    torch.float16: FSB_F16,
+    torch.bfloat16: FSB_BF16,
+    torch.float32: FSB_F32,
+    torch.float64: FSB_F64,
+    torch.complex64: FSB_C64,
+    torch.complex128: FSB_C128,
+    torch.int32: FSB_I32,
+    torch.int64: FSB_I64,
+}
+
+
+class FsbCsr(ctypes.Structure):
+    _fields_ = [
+        ("values", ctypes.c_void_p),
+        ("col_idx", ctypes.c_void_p),
+        ("row_ptr", ctypes.c_void_p),
+        ("row_map", ctypes.c_void_p),
+        ("value_dtype", ctypes.c_int32),
+        ("index_dtype", ctypes.c_int32),
+        ("ptr_dtype", ctypes.c_int32),
+        ("row_map_dtype", ctypes.c_int32),
+        ("n_rows", ctypes.c_int64),
+        ("n_cols", ctypes.c_int64),
+        ("nnz", ctypes.c_int64),
+    ]
+
+
+class FsbPlan(ctypes.Structure):
+    _fields_ = [
+        ("algo", ctypes.c_int32),
+        ("lanes", ctypes.c_int32),
+        ("items_per_unit", ctypes.c_int32),
+        ("n_tile", ctypes.c_int32),
+        ("n_units", ctypes.c_int64),
+        ("unit_coords", ctypes.c_void_p),
+        ("row_cap", ctypes.c_int64),
+        ("comp_threshold", ctypes.c_int64),
+        ("grid_blocks", ctypes.c_int32),
+        ("flags", ctypes.c_int32),
+    ]
+
+
+# name -> (restype, argtypes)
+_SIGNATURES = {
+    "fsb_abi_version": (ctypes.c_int, []),
+    "fsb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+    "fsb_last_error": (ctypes.c_char_p, []),
+    "fsb_workspace_bytes": (
+        ctypes.c_int64,
+        [ctypes.c_int, ctypes.POINTER(FsbCsr), ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(FsbPlan)],
+    ),
+    "fsb_merge_partition": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, ctypes.c_int64,
+         ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
+    ),
+    "fsb_spmv_csr": (
+        ctypes.c_int,
+        [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
+         ctypes.POINTER(FsbPlan), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
+    ),
+    "fsb_spmm_csr": (
+        ctypes.c_int,
+        [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+         ctypes.c_int, ctypes.c_int, ctypes.POINTER(FsbPlan), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
+    ),
+    "fsb_spmv_coo_atomic": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int64,
+         ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p],
+    ),
+    "fsb_spmm_coo_atomic": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int64,
+         ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
+         ctypes.c_void_p],
+    ),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+class NativeLibraryError(RuntimeError):
+    """The CUDA library is missing or failed to load."""
+
+
+def library():
+    """Load (once) and return the ctypes handle of libflagsparse_b200.so."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            raise NativeLibraryError(
+                f"{LIB_PATH} is missing: build it with `python -c 'import __graft_entry__ as g; g.build()'` "
+                "or `python flagsparse_public_b200/_build.py`; there is no non-CUDA fallback"
+            )
+        lib = ctypes.CDLL(LIB_PATH)
+        for name, (res, args) in _SIGNATURES.items():
+            fn = getattr(lib, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = lib
+    return _lib
+
+
+def declared_symbols():
+    return sorted(_SIGNATURES)
+
+
+def dtype_code(dtype):
+    try:
+        return _DTYPE_CODES[dtype]
+    except KeyError:
+        raise TypeError(f"dtype {dtype} has no kernel support") from None
+
+
+def check(status, what):
+    if status != FSB_OK:
+        lib = library()
+        msg = lib.fsb_last_error().decode(errors="replace")
+        kind = lib.fsb_status_string(status).decode()
+        raise RuntimeError(f"{what} failed ({kind}): {msg}")
+
+
+def stream_handle(device):
+    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+
+
+def ptr(t):
+    return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
+
+
+def make_csr(values, col_idx, row_ptr, n_rows, n_cols, row_map=None):
+    m = FsbCsr()
+    m.values = values.data_ptr() if values.numel() > 0 else 0
+    m.col_idx = col_idx.data_ptr() if col_idx.numel() > 0 else 0
+    m.row_ptr = row_ptr.data_ptr()
+    m.row_map = row_map.data_ptr() if row_map is not None and row_map.numel() > 0 else 0
+    m.value_dtype = dtype_code(values.dtype)
+    m.index_dtype = dtype_code(col_idx.dtype)
+    m.ptr_dtype = dtype_code(row_ptr.dtype)
+    m.row_map_dtype = dtype_code(row_map.dtype) if row_map is not None else m.index_dtype
+    m.n_rows = int(n_rows)
+    m.n_cols = int(n_cols)
+    m.nnz = int(values.numel())
+    return m
+
+
+def make_plan(algo, lanes=32, items_per_unit=0, n_tile=0, coords=None, n_units=0, row_cap=0, comp_threshold=0,
+              grid_blocks=0):
+    p = FsbPlan()
+    p.algo = int(algo)
+    p.lanes = int(lanes)
+    p.items_per_unit = int(items_per_unit)
+    p.n_tile = int(n_tile)
+    p.n_units = int(n_units)
+    p.unit_coords = coords.data_ptr() if coords is not None else 0
+    p.row_cap = int(row_cap)
+    p.comp_threshold = int(comp_threshold)
+    p.grid_blocks = int(grid_blocks)
+    p.flags = 0
+    return p

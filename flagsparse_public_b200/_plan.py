@@ -1,0 +1,190 @@
+"""Launch plans for the CSR kernels and the calls that run them.
+
+A plan names one kernel family of the C ABI (row groups or merge path) and its
+shape (lanes per row, merge-path items per unit, dense-column tile).  Plans
+come from the matrix statistics gathered at prepare time (one device->host
+read) through ``default_spmv_plan`` / ``default_spmm_plan``, or from the
+autotuner and the learned selector (``flagsparse_public_b200.tuning``).
+Merge-path partitions are computed on the device once per (matrix, plan) and
+cached on the prepared object.
+"""
+
+import math
+
+import torch
+
+from . import _native as nat
+
+SPMV_MERGE_THREADS = 128
+SPMM_SNAP_DEFAULT = 0
+
+# Kernels launched by run_spmv / run_spmm since import (partition launches
+# excluded): one per call for row groups, two (tiles + carry fix-up) for merge.
+LAUNCHES = {"count": 0}
+
+
+def _kernels_per_call(plan):
+    return 2 if plan.algo == nat.ALGO_MERGE else 1
+
+
+class MatrixStats:
+    """Row-length statistics of a CSR structure (from one host read)."""
+
+    __slots__ = ("n_rows", "n_cols", "nnz", "max_row", "mean_row", "std_row", "empty_rows")
+
+    def __init__(self, n_rows, n_cols, nnz, max_row, mean_row, std_row, empty_rows):
+        self.n_rows = int(n_rows)
+        self.n_cols = int(n_cols)
+        self.nnz = int(nnz)
+        self.max_row = int(max_row)
+        self.mean_row = float(mean_row)
+        self.std_row = float(std_row)
+        self.empty_rows = int(empty_rows)
+
+    @property
+    def skew(self):
+        return self.max_row / max(self.mean_row, 1.0)
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k in self.__slots__}
+
+
+def matrix_stats(row_ptr, n_rows, n_cols):
+    n_rows = int(n_rows)
+    if n_rows == 0:
+        return MatrixStats(0, n_cols, 0, 0, 0.0, 0.0, 0)
+    lens = (row_ptr[1:] - row_ptr[:-1]).to(torch.float64)
+    vals = torch.stack([lens.max(), lens.mean(), lens.std(unbiased=False), (lens == 0).sum().to(torch.float64),
+                        lens.sum()]).tolist()
+    return MatrixStats(n_rows, n_cols, int(vals[4]), int(vals[0]), vals[1], vals[2], int(vals[3]))
+
+
+class KernelPlan:
+    """One launch configuration of fsb_spmv_csr / fsb_spmm_csr."""
+
+    __slots__ = ("algo", "lanes", "items_per_unit", "n_tile", "snap", "coords", "n_units", "row_cap",
+                 "comp_threshold")
+
+    def __init__(self, algo, lanes=32, items_per_unit=0, n_tile=0, snap=0, row_cap=0, comp_threshold=0):
+        self.algo = int(algo)
+        self.lanes = int(lanes)
+        self.items_per_unit = int(items_per_unit)
+        self.n_tile = int(n_tile)
+        self.snap = int(snap)
+        self.coords = None
+        self.n_units = 0
+        self.row_cap = int(row_cap)
+        self.comp_threshold = int(comp_threshold)
+
+    def key(self):
+        return (self.algo, self.lanes, self.items_per_unit, self.n_tile, self.snap)
+
+    def describe(self):
+        if self.algo == nat.ALGO_ROWS:
+            kind = "warp_rows" if self.lanes == 32 else "vector_rows"
+            return {"kind": kind, "lanes": self.lanes, "n_tile": self.n_tile}
+        return {"kind": "merge_path", "items_per_unit": self.items_per_unit, "n_tile": self.n_tile,
+                "snap": self.snap, "n_units": self.n_units}
+
+    def copy(self):
+        p = KernelPlan(self.algo, self.lanes, self.items_per_unit, self.n_tile, self.snap, self.row_cap,
+                       self.comp_threshold)
+        return p
+
+    def ensure_coords(self, row_ptr, n_rows, nnz):
+        """Compute (once) the merge-path unit coordinates on the device."""
+        if self.algo != nat.ALGO_MERGE or self.coords is not None:
+            return
+        n_units = -(-(int(n_rows) + int(nnz)) // self.items_per_unit) if (n_rows + nnz) > 0 else 0
+        coords = torch.empty((n_units + 1) * 2, dtype=torch.int64, device=row_ptr.device)
+        if n_units > 0:
+            lib = nat.library()
+            rc = lib.fsb_merge_partition(nat.ptr(row_ptr), nat.dtype_code(row_ptr.dtype), int(n_rows), int(nnz),
+                                         self.items_per_unit, self.snap, nat.ptr(coords), n_units,
+                                         nat.stream_handle(row_ptr.device))
+            nat.check(rc, "fsb_merge_partition")
+        self.coords = coords
+        self.n_units = n_units
+
+    def c_plan(self):
+        return nat.make_plan(self.algo, lanes=self.lanes, items_per_unit=self.items_per_unit, n_tile=self.n_tile,
+                             coords=self.coords, n_units=self.n_units, row_cap=self.row_cap,
+                             comp_threshold=self.comp_threshold)
+
+
+def _pow2_clamp(v, lo, hi):
+    v = max(float(v), 1.0)
+    p = 1 << int(round(math.log2(v)))
+    return int(min(max(p, lo), hi))
+
+
+def _vec_elems(dtype):
+    return max(1, 16 // (torch.empty((), dtype=dtype).element_size()))
+
+
+def default_spmv_plan(stats, dtype, row_cap=0):
+    """Heuristic SpMV plan: merge path for skewed rows, else row groups sized
+    so a row's nonzeros take about one 16-byte vector per lane."""
+    if row_cap > 0 or stats.n_rows == 0:
+        lanes = _pow2_clamp(stats.mean_row / _vec_elems(dtype), 2, 32) if stats.n_rows else 32
+        return KernelPlan(nat.ALGO_ROWS, lanes=lanes, row_cap=row_cap)
+    skewed = stats.max_row > 8 * max(stats.mean_row, 1.0) + 256
+    if skewed:
+        ipt = 8 if torch.empty((), dtype=dtype).element_size() <= 4 else 4
+        return KernelPlan(nat.ALGO_MERGE, items_per_unit=SPMV_MERGE_THREADS * ipt)
+    lanes = _pow2_clamp(stats.mean_row / _vec_elems(dtype), 2, 32)
+    return KernelPlan(nat.ALGO_ROWS, lanes=lanes)
+
+
+def default_spmm_plan(stats, n_dense, dtype, row_cap=0):
+    """Heuristic SpMM plan: merge path (row-aligned units, long rows split) for
+    skewed rows; warp per row for medium rows; vector per row for short rows."""
+    if row_cap > 0 or stats.n_rows == 0:
+        return KernelPlan(nat.ALGO_ROWS, lanes=32, row_cap=row_cap)
+    skewed = stats.max_row > 8 * max(stats.mean_row, 1.0) + 64
+    if skewed:
+        return KernelPlan(nat.ALGO_MERGE, items_per_unit=128, snap=64)
+    if stats.mean_row < 6:
+        return KernelPlan(nat.ALGO_ROWS, lanes=1)  # widened to one column tile's lanes
+    return KernelPlan(nat.ALGO_ROWS, lanes=32)
+
+
+def _workspace(is_spmm, cm, n_dense, acc_mode, out_code, cp, device):
+    lib = nat.library()
+    nbytes = int(lib.fsb_workspace_bytes(int(is_spmm), cm, int(n_dense), int(acc_mode), int(out_code), cp))
+    if nbytes <= 0:
+        return None, 0
+    return torch.empty(nbytes, dtype=torch.uint8, device=device), nbytes
+
+
+def run_spmv(values, col_idx, row_ptr, n_rows, n_cols, x, y, acc_mode, plan, row_map=None):
+    """y = A x through fsb_spmv_csr on torch's current stream."""
+    if plan.algo == nat.ALGO_MERGE and plan.snap:
+        raise ValueError("SpMV merge-path tiles need an unsnapped partition (snap=0)")
+    plan.ensure_coords(row_ptr, n_rows, values.numel())
+    cm = nat.make_csr(values, col_idx, row_ptr, n_rows, n_cols, row_map)
+    cp = plan.c_plan()
+    out_code = nat.dtype_code(y.dtype)
+    ws, nbytes = _workspace(False, cm, 1, acc_mode, out_code, cp, values.device)
+    lib = nat.library()
+    rc = lib.fsb_spmv_csr(cm, nat.ptr(x), nat.ptr(y), out_code, int(acc_mode), cp, nat.ptr(ws), nbytes,
+                          nat.stream_handle(values.device))
+    nat.check(rc, "fsb_spmv_csr")
+    LAUNCHES["count"] += _kernels_per_call(plan)
+    return y
+
+
+def run_spmm(values, col_idx, row_ptr, n_rows, n_cols, B, C, acc_mode, plan, row_map=None):
+    """C = A B through fsb_spmm_csr (B, C row-major with unit column stride)."""
+    plan.ensure_coords(row_ptr, n_rows, values.numel())
+    n_dense = int(B.shape[1])
+    cm = nat.make_csr(values, col_idx, row_ptr, n_rows, n_cols, row_map)
+    cp = plan.c_plan()
+    out_code = nat.dtype_code(C.dtype)
+    ws, nbytes = _workspace(True, cm, n_dense, acc_mode, out_code, cp, values.device)
+    lib = nat.library()
+    rc = lib.fsb_spmm_csr(cm, nat.ptr(B), int(B.stride(0)), n_dense, nat.ptr(C), int(C.stride(0)), out_code,
+                          int(acc_mode), cp, nat.ptr(ws), nbytes, nat.stream_handle(values.device))
+    nat.check(rc, "fsb_spmm_csr")
+    LAUNCHES["count"] += _kernels_per_call(plan) if n_dense > 0 and n_rows > 0 else 0
+    return C

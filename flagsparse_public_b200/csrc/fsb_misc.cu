@@ -1,0 +1,195 @@
+// fsb_misc.cu -- merge-path partition, COO atomic kernels, workspace sizing and
+// error reporting of the C ABI.
+#include <stdarg.h>
+#include <stdio.h>
+
+#include "fsb_dispatch.cuh"
+
+namespace fsb_host {
+static thread_local char g_last_error[512] = "";
+
+void set_error(const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_last_error, sizeof(g_last_error), fmt, ap);
+    va_end(ap);
+}
+
+int check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        set_error("%s: %s", what, cudaGetErrorString(e));
+        return FSB_ERR_LAUNCH;
+    }
+    return FSB_OK;
+}
+}  // namespace fsb_host
+
+namespace fsb {
+
+// One thread per unit boundary u: the merge-path coordinate of diagonal
+// d = u * items, i.e. (i row ends, j nonzeros) with i + j = d, row end r
+// ordered before nonzero k iff row_ptr[r + 1] <= k.
+template <class P>
+__global__ void k_merge_partition(const P* __restrict__ ptr, int64_t n_rows, int64_t nnz, int64_t items,
+                                  int64_t snap, int64_t* __restrict__ coords, int64_t n_units) {
+    const int64_t u = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (u > n_units) return;
+    const int64_t total = n_rows + nnz;
+    int64_t d = u * items;
+    if (d > total) d = total;
+    int64_t lo = d - nnz > 0 ? d - nnz : 0;
+    int64_t hi = d < n_rows ? d : n_rows;
+    while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (idx(ptr[mid + 1]) <= d - mid - 1) lo = mid + 1; else hi = mid;
+    }
+    const int64_t i = lo;
+    int64_t j = d - lo;
+    if (snap > 0 && i < n_rows && u > 0 && u < n_units) {
+        const int64_t rs = idx(ptr[i]), re = idx(ptr[i + 1]);
+        if (j > rs && re - rs < snap) j = rs;
+    }
+    coords[2 * u] = i;
+    coords[2 * u + 1] = j;
+}
+
+template <class V, class A, class I>
+__global__ void k_spmv_coo_atomic(const V* __restrict__ val, const I* __restrict__ row, const I* __restrict__ col,
+                                  int64_t nnz, const V* __restrict__ x, A* __restrict__ y) {
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nnz) return;
+    const A p = Acc<V, A>::fma(ld_stream1(val + k), ld_ro1(x + idx(ld_stream1(col + k))), Acc<V, A>::zero());
+    atomic_accumulate(y + idx(ld_stream1(row + k)), p);
+}
+
+template <class V, class A, class I>
+__global__ void k_spmm_coo_atomic(const V* __restrict__ val, const I* __restrict__ row, const I* __restrict__ col,
+                                  int64_t nnz, const V* __restrict__ B, int64_t ldb, int64_t n_dense,
+                                  A* __restrict__ C, int64_t ldc) {
+    // One warp per nonzero, lanes over dense columns.
+    const int64_t k = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (k >= nnz) return;
+    const V a = ld_stream1(val + k);
+    const int64_t r = idx(ld_stream1(row + k)), c = idx(ld_stream1(col + k));
+    for (int64_t n = lane; n < n_dense; n += 32) {
+        const A p = Acc<V, A>::fma(a, ld_ro1(B + c * ldb + n), Acc<V, A>::zero());
+        atomic_accumulate(C + r * ldc + n, p);
+    }
+}
+
+}  // namespace fsb
+
+using namespace fsb;
+
+extern "C" int fsb_abi_version(void) { return FSB_ABI_VERSION; }
+
+extern "C" const char* fsb_status_string(int status) {
+    switch (status) {
+    case FSB_OK: return "ok";
+    case FSB_ERR_INVALID: return "invalid argument";
+    case FSB_ERR_UNSUPPORTED: return "unsupported dtype or mode";
+    case FSB_ERR_LAUNCH: return "kernel launch failed";
+    case FSB_ERR_WORKSPACE: return "workspace too small";
+    case FSB_ERR_TIMEOUT: return "device wait timed out";
+    case FSB_ERR_LIMIT: return "size exceeds entry-point limit";
+    default: return "unknown status";
+    }
+}
+
+extern "C" const char* fsb_last_error(void) { return fsb_host::g_last_error; }
+
+extern "C" int64_t fsb_workspace_bytes(int is_spmm, const fsb_csr* A, int64_t n_dense, int acc_mode, int out_dtype,
+                                       const fsb_plan* plan) {
+    (void)out_dtype;
+    if (!A || !plan || plan->algo != FSB_ALGO_MERGE) return 0;
+    const int ab = acc_size(A->value_dtype, acc_mode);
+    if (ab == 0) return 0;
+    return merge_scratch_bytes(plan->n_units, is_spmm ? n_dense : 1, ab);
+}
+
+extern "C" int fsb_merge_partition(const void* row_ptr, int ptr_dtype, int64_t n_rows, int64_t nnz,
+                                   int32_t items_per_unit, int64_t snap_threshold, int64_t* unit_coords,
+                                   int64_t n_units, void* stream) {
+    if (!row_ptr || !unit_coords || items_per_unit < 1 || n_rows < 0 || nnz < 0) {
+        fsb_host::set_error("fsb_merge_partition: bad arguments");
+        return FSB_ERR_INVALID;
+    }
+    if (n_units != ceil_div(n_rows + nnz, items_per_unit)) {
+        fsb_host::set_error("fsb_merge_partition: n_units must be ceil((n_rows + nnz) / items_per_unit)");
+        return FSB_ERR_INVALID;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return dispatch_idx(ptr_dtype, [&](auto tp) -> int {
+        using P = typename decltype(tp)::type;
+        const int64_t threads = n_units + 1;
+        k_merge_partition<P><<<(unsigned)ceil_div(threads, 256), 256, 0, st>>>(
+            static_cast<const P*>(row_ptr), n_rows, nnz, items_per_unit, snap_threshold, unit_coords, n_units);
+        return fsb_host::check_launch("k_merge_partition");
+    });
+}
+
+// Value/accumulator pairs of the atomic routes: the accumulator buffer is the
+// value type or its wide type.
+template <class F>
+static int dispatch_atomic(int vdt, int adt, F&& f) {
+    if (vdt == FSB_F32 && adt == FSB_F32) return f(tag<float>{}, tag<float>{});
+    if (vdt == FSB_F32 && adt == FSB_F64) return f(tag<float>{}, tag<double>{});
+    if (vdt == FSB_F64 && adt == FSB_F64) return f(tag<double>{}, tag<double>{});
+    if (vdt == FSB_C64 && adt == FSB_C64) return f(tag<c64_t>{}, tag<c64_t>{});
+    if (vdt == FSB_C64 && adt == FSB_C128) return f(tag<c64_t>{}, tag<c128_t>{});
+    if (vdt == FSB_C128 && adt == FSB_C128) return f(tag<c128_t>{}, tag<c128_t>{});
+    if (vdt == FSB_F16 && adt == FSB_F32) return f(tag<__half>{}, tag<float>{});
+    if (vdt == FSB_BF16 && adt == FSB_F32) return f(tag<__nv_bfloat16>{}, tag<float>{});
+    fsb_host::set_error("atomic route: unsupported value/accumulator pair (%d, %d)", vdt, adt);
+    return FSB_ERR_UNSUPPORTED;
+}
+
+extern "C" int fsb_spmv_coo_atomic(const void* values, const void* row, const void* col, int value_dtype,
+                                   int index_dtype, int64_t nnz, const void* x, void* y, int acc_dtype,
+                                   void* stream) {
+    if (nnz < 0) return FSB_ERR_INVALID;
+    if (nnz == 0) return FSB_OK;
+    if (!values || !row || !col || !x || !y) {
+        fsb_host::set_error("fsb_spmv_coo_atomic: null pointer");
+        return FSB_ERR_INVALID;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return dispatch_atomic(value_dtype, acc_dtype, [&](auto tv, auto ta) -> int {
+        using V = typename decltype(tv)::type;
+        using Ac = typename decltype(ta)::type;
+        return dispatch_idx(index_dtype, [&](auto ti) -> int {
+            using I = typename decltype(ti)::type;
+            k_spmv_coo_atomic<V, Ac, I><<<(unsigned)ceil_div(nnz, 256), 256, 0, st>>>(
+                static_cast<const V*>(values), static_cast<const I*>(row), static_cast<const I*>(col), nnz,
+                static_cast<const V*>(x), static_cast<Ac*>(y));
+            return fsb_host::check_launch("k_spmv_coo_atomic");
+        });
+    });
+}
+
+extern "C" int fsb_spmm_coo_atomic(const void* values, const void* row, const void* col, int value_dtype,
+                                   int index_dtype, int64_t nnz, const void* B, int64_t ldb, int64_t n_dense,
+                                   void* C, int64_t ldc, int acc_dtype, void* stream) {
+    if (nnz < 0 || n_dense < 0) return FSB_ERR_INVALID;
+    if (nnz == 0 || n_dense == 0) return FSB_OK;
+    if (!values || !row || !col || !B || !C) {
+        fsb_host::set_error("fsb_spmm_coo_atomic: null pointer");
+        return FSB_ERR_INVALID;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return dispatch_atomic(value_dtype, acc_dtype, [&](auto tv, auto ta) -> int {
+        using V = typename decltype(tv)::type;
+        using Ac = typename decltype(ta)::type;
+        return dispatch_idx(index_dtype, [&](auto ti) -> int {
+            using I = typename decltype(ti)::type;
+            const int64_t blocks = ceil_div(nnz, 256 / 32);
+            if (blocks > 0x7fffffffLL) return FSB_ERR_LIMIT;
+            k_spmm_coo_atomic<V, Ac, I><<<(unsigned)blocks, 256, 0, st>>>(
+                static_cast<const V*>(values), static_cast<const I*>(row), static_cast<const I*>(col), nnz,
+                static_cast<const V*>(B), ldb, n_dense, static_cast<Ac*>(C), ldc);
+            return fsb_host::check_launch("k_spmm_coo_atomic");
+        });
+    });
+}

@@ -1,0 +1,351 @@
+// fsb_spmm.cu -- CSR SpMM on sm_100a: C = A B, B and C row-major.
+//
+// Lane layout.  A dense column tile of LPN * VW columns is covered by LPN lanes
+// holding VW consecutive columns each (VW * sizeof(V) = 16 bytes when B and C
+// rows are 16-byte aligned, else VW = 1).  A group of G lanes (G a multiple of
+// LPN) works on one row; its G / LPN sub-groups take interleaved nonzeros so
+// that G / LPN B rows are in flight per step, and meet in a xor butterfly at
+// the end of the row.  Column indices and values are read once per group with
+// coalesced streaming loads and handed out by warp shuffles; B rows are
+// gathered with 16-byte read-only loads (B stays in L2), C rows are written
+// with streaming stores.
+//
+//   * k_spmm_rows  : row groups over rows (G = 32: warp per row; G = LPN:
+//                    vector per row).
+//   * k_spmm_merge : one warp per merge-path unit (rows + nonzeros balanced);
+//                    rows split across units leave a carry / head partial in
+//                    scratch that k_spmm_merge_fixup folds in, in unit order.
+//
+// FlagSparse computes the same products in _spmm_csr_real/complex_kernel
+// (spmm_csr.py:92-195), the opt bucket kernels (:602-775), the long-row split
+// kernels (:778-919), the alg2 kernels (spmm_csr_opt_alg2.py:338-629) and the
+// COO row-run kernels (spmm_coo.py:135-241).
+#include "fsb_dispatch.cuh"
+
+namespace fsb {
+
+constexpr int kSpmmThreads = 128;
+constexpr int kSpmmUnroll = 4;
+
+struct Lanes {
+    int G;       // lanes per row group
+    int LPN;     // lanes per B row (column tile)
+    int lig;     // lane in group
+    int sub;     // sub-group (nonzero slot) of this lane
+    unsigned mask;
+};
+
+template <class V, class A, class I, int VW>
+__device__ __forceinline__ void row_segment(const V* __restrict__ val, const I* __restrict__ col,
+                                            const V* __restrict__ B, int64_t ldb, int64_t c0, bool col_ok,
+                                            int64_t a, int64_t b, A (&acc)[VW], const Lanes& L) {
+    const int NPAR = L.G / L.LPN;
+    for (int64_t base = a; base < b; base += L.G) {
+        const int cnt = (b - base) < (int64_t)L.G ? (int)(b - base) : L.G;
+        V v = vzero<V>();
+        I c = 0;
+        if (L.lig < cnt) {
+            v = ld_stream1(val + base + L.lig);
+            c = ld_stream1(col + base + L.lig);
+        }
+        for (int j = 0; j < cnt; j += NPAR * kSpmmUnroll) {
+            vec_t<V, VW> bv[kSpmmUnroll];
+            V av[kSpmmUnroll];
+#pragma unroll
+            for (int u = 0; u < kSpmmUnroll; ++u) {
+                const int jj = j + u * NPAR + L.sub;
+                const V vv = shfl_idx(L.mask, v, jj & (L.G - 1), L.G);
+                const I cc = shfl_idx(L.mask, c, jj & (L.G - 1), L.G);
+                const bool ok = (jj < cnt) && col_ok;
+                av[u] = ok ? vv : vzero<V>();
+                if (ok) {
+                    bv[u] = ld_ro<V, VW>(B + idx(cc) * ldb + c0);
+                } else {
+#pragma unroll
+                    for (int w = 0; w < VW; ++w) bv[u].v[w] = vzero<V>();
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kSpmmUnroll; ++u)
+#pragma unroll
+                for (int w = 0; w < VW; ++w) acc[w] = Acc<V, A>::fma(av[u], bv[u].v[w], acc[w]);
+        }
+    }
+}
+
+template <class O, class A, int VW>
+__device__ __forceinline__ void store_row(O* __restrict__ C, int64_t ldc, int64_t out_row, int64_t c0,
+                                          const A (&acc)[VW]) {
+    if constexpr (VW > 1 && (sizeof(O) * VW == 16 || sizeof(O) * VW == 8 || sizeof(O) * VW == 4)) {
+        vec_t<O, VW> o;
+#pragma unroll
+        for (int w = 0; w < VW; ++w) o.v[w] = Out<O, A>::cvt(acc[w]);
+        st_stream<O, VW>(C + out_row * ldc + c0, o);
+    } else {
+#pragma unroll
+        for (int w = 0; w < VW; ++w) C[out_row * ldc + c0 + w] = Out<O, A>::cvt(acc[w]);
+    }
+}
+
+template <class A> struct is_comp_acc { static constexpr bool value = false; };
+template <> struct is_comp_acc<comp_t> { static constexpr bool value = true; };
+
+template <class V, class A, class I, int VW>
+__device__ __forceinline__ void row_accumulate(const V* __restrict__ val, const I* __restrict__ col,
+                                               const V* __restrict__ B, int64_t ldb, int64_t c0, bool col_ok,
+                                               int64_t a, int64_t b, int64_t row_len, int64_t comp_threshold,
+                                               A (&acc)[VW], const Lanes& L) {
+    if constexpr (is_comp_acc<A>::value) {
+        if (row_len > comp_threshold) {
+            row_segment<V, comp_t, I, VW>(val, col, B, ldb, c0, col_ok, a, b, acc, L);
+        } else {
+            float plain[VW];
+#pragma unroll
+            for (int w = 0; w < VW; ++w) plain[w] = 0.f;
+            row_segment<V, float, I, VW>(val, col, B, ldb, c0, col_ok, a, b, plain, L);
+#pragma unroll
+            for (int w = 0; w < VW; ++w) acc[w] = acc_add(acc[w], comp_t{plain[w], 0.f});
+        }
+    } else {
+        row_segment<V, A, I, VW>(val, col, B, ldb, c0, col_ok, a, b, acc, L);
+    }
+}
+
+template <class V, class A, class O, class I, class P, int VW>
+__global__ void __launch_bounds__(kSpmmThreads)
+k_spmm_rows(const V* __restrict__ val, const I* __restrict__ col, const P* __restrict__ ptr,
+            const I* __restrict__ row_map, const V* __restrict__ B, int64_t ldb, O* __restrict__ C, int64_t ldc,
+            int64_t n_rows, int64_t n_dense, int g_log2, int lpn_log2, int64_t row_cap, int64_t comp_threshold) {
+    Lanes L;
+    L.G = 1 << g_log2;
+    L.LPN = 1 << lpn_log2;
+    const int wl = threadIdx.x & 31;
+    L.lig = wl & (L.G - 1);
+    L.sub = L.lig >> lpn_log2;
+    L.mask = segment_mask(wl, L.G);
+    const int64_t c0 = (int64_t)blockIdx.y * (L.LPN * VW) + (int64_t)(L.lig & (L.LPN - 1)) * VW;
+    const bool col_ok = c0 < n_dense;
+    const int64_t stride = ((int64_t)gridDim.x * blockDim.x) >> g_log2;
+    for (int64_t row = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> g_log2; row < n_rows; row += stride) {
+        const int64_t s = idx(ptr[row]);
+        int64_t e = idx(ptr[row + 1]);
+        if (row_cap > 0 && e - s > row_cap) e = s + row_cap;
+        A acc[VW];
+#pragma unroll
+        for (int w = 0; w < VW; ++w) acc[w] = Acc<V, A>::zero();
+        row_accumulate<V, A, I, VW>(val, col, B, ldb, c0, col_ok, s, e, e - s, comp_threshold, acc, L);
+#pragma unroll
+        for (int w = 0; w < VW; ++w) acc[w] = segment_reduce(L.mask, acc[w], L.LPN, L.G);
+        if (L.sub == 0 && col_ok) {
+            const int64_t out_row = row_map ? idx(row_map[s]) : row;
+            store_row<O, A, VW>(C, ldc, out_row, c0, acc);
+        }
+    }
+}
+
+// One warp per (unit, column tile).  unit_coords as in fsb_merge_partition.
+template <class V, class A, class O, class I, class P, int VW>
+__global__ void __launch_bounds__(kSpmmThreads)
+k_spmm_merge(const V* __restrict__ val, const I* __restrict__ col, const P* __restrict__ ptr,
+             const I* __restrict__ row_map, const V* __restrict__ B, int64_t ldb, O* __restrict__ C, int64_t ldc,
+             int64_t n_rows, int64_t n_dense, int lpn_log2, const int64_t* __restrict__ coords, int64_t n_units,
+             int64_t comp_threshold, int64_t* __restrict__ carry_row, A* __restrict__ carry_val,
+             A* __restrict__ head_val) {
+    const int64_t unit = (int64_t)blockIdx.x * (kSpmmThreads / 32) + (threadIdx.x >> 5);
+    if (unit >= n_units) return;
+    Lanes L;
+    L.G = 32;
+    L.LPN = 1 << lpn_log2;
+    L.lig = threadIdx.x & 31;
+    L.sub = L.lig >> lpn_log2;
+    L.mask = 0xffffffffu;
+    const int64_t c0 = (int64_t)blockIdx.y * (L.LPN * VW) + (int64_t)(L.lig & (L.LPN - 1)) * VW;
+    const bool col_ok = c0 < n_dense;
+
+    const int64_t r0 = coords[2 * unit], k0 = coords[2 * unit + 1];
+    const int64_t r1 = coords[2 * unit + 2], k1 = coords[2 * unit + 3];
+    const int64_t last = r1 < n_rows ? r1 : r1 - 1;
+    int64_t s_next = r0 < n_rows ? idx(ptr[r0]) : k1;
+    const bool continued = (r0 < n_rows) && (k0 > s_next);
+    bool open = false;
+    for (int64_t r = r0; r <= last; ++r) {
+        const int64_t rs = s_next;
+        const int64_t re_full = idx(ptr[r + 1]);
+        s_next = re_full;
+        const int64_t a = rs > k0 ? rs : k0;
+        const int64_t b = (r < r1) ? re_full : k1;
+        if (r == r1 && b <= a) break;  // open row untouched by this unit
+        A acc[VW];
+#pragma unroll
+        for (int w = 0; w < VW; ++w) acc[w] = Acc<V, A>::zero();
+        row_accumulate<V, A, I, VW>(val, col, B, ldb, c0, col_ok, a, b, re_full - rs, comp_threshold, acc, L);
+#pragma unroll
+        for (int w = 0; w < VW; ++w) acc[w] = segment_reduce(L.mask, acc[w], L.LPN, 32);
+        if (L.sub == 0 && col_ok) {
+            if (r == r1) {
+                A* dst = carry_val + unit * n_dense + c0;
+#pragma unroll
+                for (int w = 0; w < VW; ++w) dst[w] = acc[w];
+            } else if (r == r0 && continued) {
+                A* dst = head_val + unit * n_dense + c0;
+#pragma unroll
+                for (int w = 0; w < VW; ++w) dst[w] = acc[w];
+            } else {
+                const int64_t out_row = row_map ? idx(row_map[rs]) : r;
+                store_row<O, A, VW>(C, ldc, out_row, c0, acc);
+            }
+        }
+        if (r == r1) open = true;
+    }
+    if (blockIdx.y == 0 && L.lig == 0) carry_row[unit] = open ? r1 : -1;
+}
+
+// One warp per unit: the first unit of each run carrying the same open row
+// folds the run's carries (unit order) and the ending unit's head partial.
+template <class A, class O, class I, class P>
+__global__ void __launch_bounds__(kSpmmThreads)
+k_spmm_merge_fixup(const int64_t* __restrict__ carry_row, const A* __restrict__ carry_val,
+                   const A* __restrict__ head_val, int64_t n_units, int64_t n_dense, const P* __restrict__ ptr,
+                   const I* __restrict__ row_map, O* __restrict__ C, int64_t ldc) {
+    const int64_t t = (int64_t)blockIdx.x * (kSpmmThreads / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (t >= n_units) return;
+    const int64_t r = carry_row[t];
+    if (r < 0) return;
+    if (t > 0 && carry_row[t - 1] == r) return;
+    int64_t u_end = t + 1;
+    while (u_end < n_units && carry_row[u_end] == r) ++u_end;
+    const int64_t out_row = row_map ? idx(row_map[idx(ptr[r])]) : r;
+    for (int64_t c = lane; c < n_dense; c += 32) {
+        A sum = carry_val[t * n_dense + c];
+        for (int64_t u = t + 1; u < u_end; ++u) sum = acc_add(sum, carry_val[u * n_dense + c]);
+        if (u_end < n_units) sum = acc_add(sum, head_val[u_end * n_dense + c]);
+        C[out_row * ldc + c] = Out<O, A>::cvt(sum);
+    }
+}
+
+template <class V, class A, class O, class I, class P, int VW>
+int launch_spmm(const fsb_csr* Am, const V* val, const I* col, const P* ptr, const I* rmap, const V* B, int64_t ldb,
+                int64_t n_dense, O* C, int64_t ldc, const fsb_plan* plan, void* workspace, int64_t workspace_bytes,
+                cudaStream_t st) {
+    int ntile = plan->n_tile > 0 ? plan->n_tile : (int)(n_dense < 32 * VW ? n_dense : 32 * VW);
+    int lpn = (int)ceil_div(ntile, VW);
+    int lpn_log2 = 0;
+    while ((1 << lpn_log2) < lpn && lpn_log2 < 5) ++lpn_log2;
+    lpn = 1 << lpn_log2;
+    const int64_t col_tiles = ceil_div(n_dense, (int64_t)lpn * VW);
+    if (col_tiles > 65535) {
+        fsb_host::set_error("fsb_spmm_csr: too many column tiles");
+        return FSB_ERR_LIMIT;
+    }
+    const int64_t thr = plan->comp_threshold > 0 ? plan->comp_threshold : 0;
+    if (plan->algo == FSB_ALGO_ROWS) {
+        int G = plan->lanes;
+        if (G < 1 || G > 32 || (G & (G - 1))) {
+            fsb_host::set_error("fsb_spmm_csr: lanes=%d is not a power of two in [1, 32]", G);
+            return FSB_ERR_INVALID;
+        }
+        if (G < lpn) G = lpn;
+        int g_log2 = 0;
+        while ((1 << g_log2) < G) ++g_log2;
+        int64_t grid = ceil_div(Am->n_rows, kSpmmThreads / G);
+        if (plan->grid_blocks > 0 && grid > plan->grid_blocks) grid = plan->grid_blocks;
+        if (grid > 0x7fffffffLL) grid = 0x7fffffffLL;
+        dim3 g((unsigned)grid, (unsigned)col_tiles);
+        k_spmm_rows<V, A, O, I, P, VW><<<g, kSpmmThreads, 0, st>>>(val, col, ptr, rmap, B, ldb, C, ldc, Am->n_rows,
+                                                                   n_dense, g_log2, lpn_log2, plan->row_cap, thr);
+        return fsb_host::check_launch("k_spmm_rows");
+    }
+    if (plan->algo != FSB_ALGO_MERGE) {
+        fsb_host::set_error("fsb_spmm_csr: unknown algo %d", plan->algo);
+        return FSB_ERR_INVALID;
+    }
+    const int64_t n_units = plan->n_units;
+    if (plan->items_per_unit < 1 || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
+        !plan->unit_coords) {
+        fsb_host::set_error("fsb_spmm_csr: merge plan does not match the matrix");
+        return FSB_ERR_INVALID;
+    }
+    if (plan->row_cap > 0) {
+        fsb_host::set_error("fsb_spmm_csr: row_cap needs the rows algorithm");
+        return FSB_ERR_INVALID;
+    }
+    const int64_t need = merge_scratch_bytes(n_units, n_dense, (int)sizeof(A));
+    if (!workspace || workspace_bytes < need) {
+        fsb_host::set_error("fsb_spmm_csr: workspace %lld bytes < %lld", (long long)workspace_bytes, (long long)need);
+        return FSB_ERR_WORKSPACE;
+    }
+    MergeScratch ms = merge_scratch_carve(workspace, n_units, n_dense, (int)sizeof(A));
+    const int64_t blocks = ceil_div(n_units, kSpmmThreads / 32);
+    if (blocks > 0x7fffffffLL) {
+        fsb_host::set_error("fsb_spmm_csr: too many merge units");
+        return FSB_ERR_LIMIT;
+    }
+    dim3 g((unsigned)blocks, (unsigned)col_tiles);
+    k_spmm_merge<V, A, O, I, P, VW><<<g, kSpmmThreads, 0, st>>>(
+        val, col, ptr, rmap, B, ldb, C, ldc, Am->n_rows, n_dense, lpn_log2, plan->unit_coords, n_units, thr,
+        ms.carry_row, static_cast<A*>(ms.carry_val), static_cast<A*>(ms.head_val));
+    int rc = fsb_host::check_launch("k_spmm_merge");
+    if (rc) return rc;
+    k_spmm_merge_fixup<A, O, I, P><<<(unsigned)blocks, kSpmmThreads, 0, st>>>(
+        ms.carry_row, static_cast<const A*>(ms.carry_val), static_cast<const A*>(ms.head_val), n_units, n_dense, ptr,
+        rmap, C, ldc);
+    return fsb_host::check_launch("k_spmm_merge_fixup");
+}
+
+}  // namespace fsb
+
+using namespace fsb;
+
+extern "C" int fsb_spmm_csr(const fsb_csr* A, const void* B, int64_t ldb, int64_t n_dense, void* C, int64_t ldc,
+                            int out_dtype, int acc_mode, const fsb_plan* plan, void* workspace,
+                            int64_t workspace_bytes, void* stream) {
+    if (!A || !plan) {
+        fsb_host::set_error("fsb_spmm_csr: null matrix or plan");
+        return FSB_ERR_INVALID;
+    }
+    if (A->n_rows < 0 || A->nnz < 0 || n_dense < 0 || ldb < n_dense || ldc < n_dense) {
+        fsb_host::set_error("fsb_spmm_csr: bad sizes");
+        return FSB_ERR_INVALID;
+    }
+    if (A->n_rows == 0 || n_dense == 0) return FSB_OK;
+    if (!A->row_ptr || !C || (A->nnz > 0 && (!A->values || !A->col_idx || !B))) {
+        fsb_host::set_error("fsb_spmm_csr: null data pointer");
+        return FSB_ERR_INVALID;
+    }
+    if (A->row_map && A->row_map_dtype != A->index_dtype) {
+        fsb_host::set_error("fsb_spmm_csr: row_map dtype must equal index dtype");
+        return FSB_ERR_INVALID;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return dispatch_vao(A->value_dtype, acc_mode, out_dtype, [&](auto tv, auto ta, auto to) -> int {
+        using V = typename decltype(tv)::type;
+        using Ac = typename decltype(ta)::type;
+        using O = typename decltype(to)::type;
+        return dispatch_idx(A->index_dtype, [&](auto ti) -> int {
+            using I = typename decltype(ti)::type;
+            return dispatch_idx(A->ptr_dtype, [&](auto tp) -> int {
+                using P = typename decltype(tp)::type;
+                constexpr int VW = VecWidth<V>::value < VecWidth<O>::value ? VecWidth<V>::value
+                                                                           : VecWidth<O>::value;
+                const V* val = static_cast<const V*>(A->values);
+                const I* col = static_cast<const I*>(A->col_idx);
+                const P* ptr = static_cast<const P*>(A->row_ptr);
+                const I* rmap = static_cast<const I*>(A->row_map);
+                const V* Bv = static_cast<const V*>(B);
+                O* Cv = static_cast<O*>(C);
+                // 16-byte vectors need aligned bases and row strides; the output
+                // vector must be a loadable width too.
+                const bool vec_ok = VW > 1 && aligned16(Bv) && (ldb % VW == 0) && (n_dense % VW == 0) &&
+                                    (((uintptr_t)Cv) % (sizeof(O) * VW) == 0) && (ldc % VW == 0) &&
+                                    (sizeof(O) * VW <= 16);
+                if (vec_ok)
+                    return launch_spmm<V, Ac, O, I, P, (VW > 1 ? VW : 1)>(A, val, col, ptr, rmap, Bv, ldb, n_dense,
+                                                                          Cv, ldc, plan, workspace, workspace_bytes,
+                                                                          st);
+                return launch_spmm<V, Ac, O, I, P, 1>(A, val, col, ptr, rmap, Bv, ldb, n_dense, Cv, ldc, plan,
+                                                      workspace, workspace_bytes, st);
+            });
+        });
+    });
+}

@@ -1,0 +1,157 @@
+/*
+ * flagsparse_b200.h -- C ABI of the B200 (sm_100a) sparse-matrix kernels.
+ *
+ * Every entry point takes plain device pointers, element counts and a CUDA
+ * stream handle (cudaStream_t passed as void*), enqueues its kernels on that
+ * stream and returns a status code.  No entry point allocates device memory,
+ * synchronises the stream or reads device data on the host: scratch memory is
+ * passed in by the caller (its size comes from fsb_workspace_bytes).
+ *
+ * The Python package flagsparse_public_b200 binds these through ctypes and
+ * keeps the FlagSparse operator API (prepare_* / flagsparse_* functions) on
+ * top.  Each declaration names the FlagSparse launch it replaces; paths are
+ * relative to the FlagSparse project root.
+ */
+#ifndef FLAGSPARSE_B200_H
+#define FLAGSPARSE_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FSB_ABI_VERSION 1
+
+/* ---- status codes ------------------------------------------------------ */
+#define FSB_OK               0
+#define FSB_ERR_INVALID     -1  /* bad argument (null pointer, bad size, bad plan) */
+#define FSB_ERR_UNSUPPORTED -2  /* dtype / mode combination not compiled in       */
+#define FSB_ERR_LAUNCH      -3  /* cudaGetLastError() reported a launch failure    */
+#define FSB_ERR_WORKSPACE   -4  /* workspace missing or smaller than required      */
+#define FSB_ERR_TIMEOUT     -5  /* a bounded device wait gave up                   */
+#define FSB_ERR_LIMIT       -6  /* size exceeds a fixed limit of the entry point   */
+
+/* ---- element type codes ------------------------------------------------ */
+#define FSB_F16   0
+#define FSB_BF16  1
+#define FSB_F32   2
+#define FSB_F64   3
+#define FSB_C64   4   /* interleaved (re, im) float pairs  */
+#define FSB_C128  5   /* interleaved (re, im) double pairs */
+#define FSB_I32   6
+#define FSB_I64   7
+
+/* ---- accumulation modes ------------------------------------------------
+ * NATIVE : f16/bf16 -> f32, f32 -> f32, f64 -> f64, c64 -> f32 pairs
+ *          (the FlagSparse "opt" paths: spmv_csr.py:246, spmm_csr.py:631)
+ * WIDE   : f16/bf16 -> f32, f32 -> f64, c64 -> f64 pairs, f64 -> f64
+ *          (the FlagSparse plain paths: spmv_csr.py:116-121,
+ *           spmm_csr.py:544-551, spmm_coo.py:11-18)
+ * COMP   : f16/bf16/f32 values, f32 accumulation with error-free
+ *          transformations (TwoProduct by FMA + TwoSum, Ogita-Rump-Oishi
+ *          Dot2) on rows longer than plan->comp_threshold nonzeros.      */
+#define FSB_ACC_NATIVE 0
+#define FSB_ACC_WIDE   1
+#define FSB_ACC_COMP   2
+
+/* ---- algorithms ------------------------------------------------------- */
+#define FSB_ALGO_ROWS   0  /* one group of plan->lanes lanes per row        */
+#define FSB_ALGO_MERGE  1  /* merge-path units over (rows + nonzeros)      */
+
+/* A CSR matrix (or a sorted COO matrix seen as row runs).
+ * row_ptr has n_rows + 1 entries.  If row_map is non-null, row r of this
+ * structure is written to output row row_map[row_ptr[r]] (COO row runs:
+ * row_ptr = seg_starts, row_map = the sorted COO row array).              */
+typedef struct fsb_csr {
+    const void* values;
+    const void* col_idx;
+    const void* row_ptr;
+    const void* row_map;
+    int32_t value_dtype;    /* FSB_F16 .. FSB_C128 */
+    int32_t index_dtype;    /* FSB_I32 / FSB_I64, col_idx */
+    int32_t ptr_dtype;      /* FSB_I32 / FSB_I64, row_ptr */
+    int32_t row_map_dtype;  /* FSB_I32 / FSB_I64, row_map */
+    int64_t n_rows;
+    int64_t n_cols;
+    int64_t nnz;
+} fsb_csr;
+
+/* Launch plan chosen by the host (heuristic, autotuner or learned selector). */
+typedef struct fsb_plan {
+    int32_t algo;            /* FSB_ALGO_ROWS / FSB_ALGO_MERGE                     */
+    int32_t lanes;           /* ROWS: lanes per row group, power of two in [1, 32] */
+    int32_t items_per_unit;  /* MERGE: path items (rows + nnz) per unit           */
+    int32_t n_tile;          /* SpMM: dense columns per column tile, 0 = all       */
+    int64_t n_units;         /* MERGE: number of units                             */
+    const int64_t* unit_coords; /* MERGE: device array [(n_units + 1) * 2] of
+                                   (row, nnz) unit start coordinates              */
+    int64_t row_cap;         /* > 0: nonzeros consumed per row are capped
+                                (FlagSparse max_segments * block_nnz)             */
+    int64_t comp_threshold;  /* FSB_ACC_COMP: rows longer than this are
+                                compensated (FlagSparse precision form: 4096)     */
+    int32_t grid_blocks;     /* ROWS: CTAs to launch, 0 = automatic                */
+    int32_t flags;           /* reserved, 0                                         */
+} fsb_plan;
+
+int         fsb_abi_version(void);
+const char* fsb_status_string(int status);
+/* Text of the last error recorded by this thread (launch errors, bad plans). */
+const char* fsb_last_error(void);
+
+/* Scratch bytes fsb_spmv_csr / fsb_spmm_csr need for this plan (0 for ROWS). */
+int64_t fsb_workspace_bytes(int is_spmm, const fsb_csr* A, int64_t n_dense,
+                            int acc_mode, int out_dtype, const fsb_plan* plan);
+
+/* Merge-path partition: unit_coords[2*u], unit_coords[2*u+1] = (row, nnz)
+ * coordinate of path diagonal u * items_per_unit, for u in [0, n_units], the
+ * last one clamped to (n_rows, nnz).  With snap_threshold > 0 a boundary that
+ * falls inside a row shorter than snap_threshold nonzeros is moved back to the
+ * start of that row (fewer split rows).  n_units must be
+ * ceil((n_rows + nnz) / items_per_unit).
+ * Replaces the host-side long-row split of spmm_csr.py:417-441 and the
+ * per-bucket torch.nonzero launches of spmv_csr.py:345-391.               */
+int fsb_merge_partition(const void* row_ptr, int ptr_dtype, int64_t n_rows,
+                        int64_t nnz, int32_t items_per_unit,
+                        int64_t snap_threshold, int64_t* unit_coords,
+                        int64_t n_units, void* stream);
+
+/* y = A x.  out_dtype is value_dtype, or FSB_F32 for f16/bf16 values (the
+ * precision form).  y must be zero-filled by the caller when row_map is set
+ * (rows without a run are not written).
+ * Replaces the launches of _spmv_csr_real_kernel / _spmv_csr_complex_kernel
+ * (spmv_csr.py:677-705), the bucket kernels of
+ * _triton_spmv_csr_impl_opt_prepared (spmv_csr.py:403-439) and the row-run
+ * kernels _spmv_coo_seg_* (spmv_coo.py:436-478).                          */
+int fsb_spmv_csr(const fsb_csr* A, const void* x, void* y, int out_dtype,
+                 int acc_mode, const fsb_plan* plan, void* workspace,
+                 int64_t workspace_bytes, void* stream);
+
+/* C[:, :n_dense] = A B with B row-major (n_cols x n_dense, row stride ldb
+ * elements) and C row-major (n_rows x n_dense, row stride ldc elements).
+ * Replaces _spmm_csr_real/complex_kernel (spmm_csr.py:553-598), the opt
+ * bucket and split kernels (spmm_csr.py:1252-1360), the alg2 kernels
+ * (spmm_csr_opt_alg2.py:684-768) and the COO row-run kernels
+ * (spmm_coo.py:415-460).                                                  */
+int fsb_spmm_csr(const fsb_csr* A, const void* B, int64_t ldb, int64_t n_dense,
+                 void* C, int64_t ldc, int out_dtype, int acc_mode,
+                 const fsb_plan* plan, void* workspace, int64_t workspace_bytes,
+                 void* stream);
+
+/* Unsorted COO, one atomic add per product into a zero-filled y / C whose
+ * element type acc_dtype is the value type or its wide type (f32 -> f64,
+ * c64 -> c128); products are formed in acc_dtype.  Order not deterministic.
+ * Replaces _spmv_coo_atomic_* (spmv_coo.py:229-294, launched at :451-491)
+ * and _spmm_coo_atomic_* (spmm_coo.py:243-311, launched at :487-522).     */
+int fsb_spmv_coo_atomic(const void* values, const void* row, const void* col,
+                        int value_dtype, int index_dtype, int64_t nnz,
+                        const void* x, void* y, int acc_dtype, void* stream);
+int fsb_spmm_coo_atomic(const void* values, const void* row, const void* col,
+                        int value_dtype, int index_dtype, int64_t nnz,
+                        const void* B, int64_t ldb, int64_t n_dense, void* C,
+                        int64_t ldc, int acc_dtype, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FLAGSPARSE_B200_H */

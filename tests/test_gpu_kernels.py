@@ -1,0 +1,209 @@
+"""Every kernel family of the C ABI against the FP64 oracle.
+
+Each launch goes through ``fsb_spmv_csr`` / ``fsb_spmm_csr`` with an explicit
+plan (row groups of 1..32 lanes, merge-path tiles/units of several sizes,
+column tiles), on matrices that stress row-boundary handling: empty rows,
+rows of 1/31/32/33/4095/4097 nonzeros, heavy skew, all-empty matrices.
+
+Bounds (condition-scaled, see tests/numerics.py): float32 with float64
+accumulation within 1e-5 and within one float32 rounding of the FP64 result;
+float32 accumulation within 3e-5; float64 within 1e-12; half types within
+one rounding of the output type.
+"""
+
+import pytest
+import torch
+
+from flagsparse_public_b200 import _native as nat
+from flagsparse_public_b200 import _plan
+from oracle import oracle as orc
+from tests.gpu_cases import EDGE_LENGTHS, csr_from_lengths, dense, spmm_plans, spmv_plans
+from tests.numerics import REL_BOUND, scaled_error, ulp_distance_f32
+
+pytestmark = pytest.mark.gpu
+DEV = "cuda"
+
+NATIVE_F32_BOUND = 3e-5
+
+# (value dtype, acc mode, output dtype, bound)
+SPMV_MODES = [
+    (torch.float32, nat.ACC_WIDE, torch.float32, REL_BOUND[torch.float32]),
+    (torch.float32, nat.ACC_NATIVE, torch.float32, NATIVE_F32_BOUND),
+    (torch.float64, nat.ACC_NATIVE, torch.float64, REL_BOUND[torch.float64]),
+    (torch.float16, nat.ACC_NATIVE, torch.float16, REL_BOUND[torch.float16]),
+    (torch.bfloat16, nat.ACC_NATIVE, torch.bfloat16, REL_BOUND[torch.bfloat16]),
+    (torch.bfloat16, nat.ACC_NATIVE, torch.float32, NATIVE_F32_BOUND),
+    (torch.complex64, nat.ACC_NATIVE, torch.complex64, NATIVE_F32_BOUND),
+    (torch.complex64, nat.ACC_WIDE, torch.complex64, REL_BOUND[torch.complex64]),
+    (torch.complex128, nat.ACC_NATIVE, torch.complex128, REL_BOUND[torch.complex128]),
+]
+
+
+def _mode_id(m):
+    return f"{str(m[0])[6:]}-{['native', 'wide', 'comp'][m[1]]}-{str(m[2])[6:]}"
+
+
+@pytest.mark.parametrize("pattern", sorted(EDGE_LENGTHS))
+@pytest.mark.parametrize("mode", SPMV_MODES, ids=_mode_id)
+def test_spmv_all_plans_edge_patterns(pattern, mode):
+    dtype, acc, out_dtype, bound = mode
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths(EDGE_LENGTHS[pattern], 13000, seed=5, dtype=dtype)
+    x = dense((n_cols,), 6, dtype)
+    exact, mag = orc.spmv_csr_exact(data, indices, indptr, x)
+    d_data, d_idx, d_ptr, d_x = data.to(DEV), indices.to(DEV), indptr.to(DEV), x.to(DEV)
+    for plan in spmv_plans(dtype):
+        y = torch.full((n_rows,), float("nan"), dtype=out_dtype, device=DEV)
+        _plan.run_spmv(d_data, d_idx, d_ptr, n_rows, n_cols, d_x, y, acc, plan)
+        err = scaled_error(y, exact, mag)
+        assert err <= bound, (plan.describe(), err)
+        if dtype == torch.float32 and acc == nat.ACC_WIDE:
+            assert ulp_distance_f32(y.cpu(), exact.to(torch.float32)) <= 1, plan.describe()
+
+
+@pytest.mark.parametrize("index_dtype,ptr_dtype", [(torch.int32, torch.int32), (torch.int32, torch.int64),
+                                                   (torch.int64, torch.int32), (torch.int64, torch.int64)])
+def test_spmv_index_widths(index_dtype, ptr_dtype):
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths(EDGE_LENGTHS["skewed"], 20000, seed=7,
+                                                               index_dtype=index_dtype, ptr_dtype=ptr_dtype)
+    x = dense((n_cols,), 8, torch.float32)
+    exact, mag = orc.spmv_csr_exact(data, indices, indptr, x)
+    for plan in spmv_plans(torch.float32):
+        y = torch.empty(n_rows, dtype=torch.float32, device=DEV)
+        _plan.run_spmv(data.to(DEV), indices.to(DEV), indptr.to(DEV), n_rows, n_cols, x.to(DEV), y, nat.ACC_WIDE,
+                       plan)
+        assert scaled_error(y, exact, mag) <= 1e-5
+
+
+def test_spmv_unaligned_views_use_scalar_path():
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths([5, 9, 17, 33, 64, 3], 100, seed=9)
+    # shift the arrays by one element so 16-byte vector loads are not allowed
+    data_u = torch.cat([torch.zeros(1), data]).to(DEV)[1:]
+    idx_u = torch.cat([torch.zeros(1, dtype=torch.int32), indices]).to(DEV)[1:]
+    x = dense((n_cols,), 10, torch.float32)
+    exact, mag = orc.spmv_csr_exact(data, indices, indptr, x)
+    for lanes in (2, 4, 32):
+        y = torch.empty(n_rows, device=DEV)
+        _plan.run_spmv(data_u, idx_u, indptr.to(DEV), n_rows, n_cols, x.to(DEV), y, nat.ACC_WIDE,
+                       _plan.KernelPlan(nat.ALGO_ROWS, lanes=lanes))
+        assert scaled_error(y, exact, mag) <= 1e-5
+
+
+def test_spmv_row_cap_truncates_like_reference_window():
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths([10, 40, 70, 0, 33], 200, seed=11)
+    x = dense((n_cols,), 12, torch.float32)
+    ref = orc.spmv_csr(data, indices, indptr, x, acc_mode=orc.ACC_WIDE, row_cap=32)
+    y = torch.empty(n_rows, device=DEV)
+    _plan.run_spmv(data.to(DEV), indices.to(DEV), indptr.to(DEV), n_rows, n_cols, x.to(DEV), y, nat.ACC_WIDE,
+                   _plan.KernelPlan(nat.ALGO_ROWS, lanes=8, row_cap=32))
+    assert ulp_distance_f32(y.cpu(), ref) <= 1
+
+
+def test_spmv_row_map_runs():
+    """Row runs of sorted COO: row_ptr = run offsets, output row = row_map[start]."""
+    rows = torch.tensor([1, 1, 4, 4, 4, 7, 9, 9], dtype=torch.int32)
+    cols = torch.tensor([0, 5, 1, 2, 9, 3, 0, 8], dtype=torch.int32)
+    vals = dense((8,), 13, torch.float64)
+    x = dense((10,), 14, torch.float64)
+    seg = torch.tensor([0, 2, 5, 6, 8], dtype=torch.int32)
+    ref = torch.zeros(10, dtype=torch.float64).index_add_(0, rows.long(), vals * x[cols.long()])
+    for plan in spmv_plans(torch.float64):
+        y = torch.zeros(10, dtype=torch.float64, device=DEV)
+        _plan.run_spmv(vals.to(DEV), cols.to(DEV), seg.to(DEV), 4, 10, x.to(DEV), y, nat.ACC_NATIVE, plan,
+                       row_map=rows.to(DEV))
+        assert torch.allclose(y.cpu(), ref, rtol=1e-13, atol=1e-14), plan.describe()
+
+
+@pytest.mark.parametrize("vdtype", [torch.bfloat16, torch.float16, torch.float32])
+def test_spmv_compensated_long_rows(vdtype):
+    """COMP accumulation: rows > threshold carry a TwoSum/TwoProduct error term."""
+    lengths = [8192] * 8 + [68] * 200 + [5000, 9000]
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths(lengths, 12000, seed=15, dtype=vdtype)
+    x = dense((n_cols,), 16, vdtype)
+    exact, mag = orc.spmv_csr_exact(data, indices, indptr, x)
+    for plan in (_plan.KernelPlan(nat.ALGO_ROWS, lanes=32, comp_threshold=4096),
+                 _plan.KernelPlan(nat.ALGO_MERGE, items_per_unit=1024, comp_threshold=4096)):
+        y = torch.empty(n_rows, dtype=torch.float32, device=DEV)
+        _plan.run_spmv(data.to(DEV), indices.to(DEV), indptr.to(DEV), n_rows, n_cols, x.to(DEV), y, nat.ACC_COMP,
+                       plan)
+        lens = (indptr[1:] - indptr[:-1])
+        long_rows = lens > 4096
+        err_long = scaled_error(y.cpu()[long_rows], exact[long_rows], mag[long_rows])
+        assert err_long <= 2e-7, (plan.describe(), err_long)
+        assert scaled_error(y, exact, mag) <= NATIVE_F32_BOUND
+
+
+SPMM_MODES = [
+    (torch.float32, nat.ACC_WIDE, torch.float32, REL_BOUND[torch.float32]),
+    (torch.float32, nat.ACC_NATIVE, torch.float32, NATIVE_F32_BOUND),
+    (torch.float64, nat.ACC_NATIVE, torch.float64, REL_BOUND[torch.float64]),
+    (torch.float16, nat.ACC_NATIVE, torch.float16, REL_BOUND[torch.float16]),
+    (torch.bfloat16, nat.ACC_NATIVE, torch.float32, NATIVE_F32_BOUND),
+    (torch.complex64, nat.ACC_NATIVE, torch.complex64, NATIVE_F32_BOUND),
+    (torch.complex64, nat.ACC_WIDE, torch.complex64, REL_BOUND[torch.complex64]),
+    (torch.complex128, nat.ACC_NATIVE, torch.complex128, REL_BOUND[torch.complex128]),
+]
+
+
+@pytest.mark.parametrize("pattern", ["empty_rows", "boundaries", "skewed", "all_empty", "one_row"])
+@pytest.mark.parametrize("n_dense", [1, 3, 8, 32, 64, 96])
+@pytest.mark.parametrize("mode", SPMM_MODES, ids=_mode_id)
+def test_spmm_all_plans(pattern, n_dense, mode):
+    dtype, acc, out_dtype, bound = mode
+    lengths = EDGE_LENGTHS[pattern]
+    if pattern == "skewed":
+        lengths = lengths[::3]
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths(lengths, 13000, seed=17, dtype=dtype)
+    B = dense((n_cols, n_dense), 18, dtype)
+    exact, mag = orc.spmm_csr_exact(data, indices, indptr, B)
+    d = (data.to(DEV), indices.to(DEV), indptr.to(DEV))
+    Bd = B.to(DEV)
+    for plan in spmm_plans():
+        C = torch.full((n_rows, n_dense), float("nan"), dtype=out_dtype, device=DEV)
+        _plan.run_spmm(*d, n_rows, n_cols, Bd, C, acc, plan)
+        err = scaled_error(C, exact, mag)
+        assert err <= bound, (plan.describe(), err)
+
+
+def test_spmm_strided_output_and_operand():
+    """ldb / ldc larger than the dense width (views into wider buffers)."""
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths([3, 0, 40, 7, 300], 500, seed=19)
+    Bw = dense((n_cols, 80), 20, torch.float32)
+    B = Bw[:, :64]
+    exact, mag = orc.spmm_csr_exact(data, indices, indptr, B.contiguous())
+    Cw = torch.zeros((n_rows, 72), device=DEV)
+    C = Cw[:, :64]
+    lib = nat.library()
+    cm = nat.make_csr(data.to(DEV), indices.to(DEV), indptr.to(DEV), n_rows, n_cols)
+    Bd = Bw.to(DEV)
+    cp = _plan.KernelPlan(nat.ALGO_ROWS, lanes=32).c_plan()
+    rc = lib.fsb_spmm_csr(cm, nat.ptr(Bd), 80, 64, nat.ptr(Cw), 72, nat.FSB_F32, nat.ACC_WIDE, cp, None, 0,
+                          nat.stream_handle(torch.device(DEV)))
+    nat.check(rc, "fsb_spmm_csr")
+    assert scaled_error(C, exact, mag) <= 1e-5
+    assert bool((Cw[:, 64:] == 0).all()), "columns beyond n_dense were written"
+
+
+def test_spmm_compensated_long_rows():
+    lengths = [8192] * 4 + [68] * 100 + [6000]
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths(lengths, 12000, seed=21, dtype=torch.bfloat16)
+    B = dense((n_cols, 32), 22, torch.bfloat16)
+    exact, mag = orc.spmm_csr_exact(data, indices, indptr, B)
+    lens = indptr[1:] - indptr[:-1]
+    long_rows = lens > 4096
+    for plan in (_plan.KernelPlan(nat.ALGO_ROWS, lanes=32, comp_threshold=4096),
+                 _plan.KernelPlan(nat.ALGO_MERGE, items_per_unit=256, snap=64, comp_threshold=4096)):
+        C = torch.empty((n_rows, 32), dtype=torch.float32, device=DEV)
+        _plan.run_spmm(data.to(DEV), indices.to(DEV), indptr.to(DEV), n_rows, n_cols, B.to(DEV), C, nat.ACC_COMP,
+                       plan)
+        err_long = scaled_error(C.cpu()[long_rows], exact[long_rows], mag[long_rows])
+        assert err_long <= 2e-7, (plan.describe(), err_long)
+
+
+def test_merge_partition_kernel_matches_oracle():
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths(EDGE_LENGTHS["skewed"], 20000, seed=23)
+    nnz = data.numel()
+    for items, snap in ((128, 0), (256, 64), (1024, 0), (77, 30)):
+        plan = _plan.KernelPlan(nat.ALGO_MERGE, items_per_unit=items, snap=snap)
+        plan.ensure_coords(indptr.to(DEV), n_rows, nnz)
+        ref = orc.merge_partition(indptr, n_rows, nnz, items, snap)
+        assert torch.equal(plan.coords.cpu(), ref)

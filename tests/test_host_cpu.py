@@ -1,0 +1,181 @@
+"""Host-side logic of the drop-in operators, on CPU tensors (no kernel runs).
+
+Covers the integer preparation steps that must reproduce FlagSparse's
+structure bit for bit (golden fixtures), the validation errors raised before
+any device work, the int64 -> int32 fallback policy (failure injected on the
+host, as FlagSparse's own tests do) and the default kernel plans.
+"""
+
+import pytest
+import torch
+
+import flagsparse_public_b200.sparse_operations.spmm_coo as spmm_coo_mod
+import flagsparse_public_b200.sparse_operations.spmm_csr as spmm_mod
+import flagsparse_public_b200.sparse_operations.spmv_coo as spmv_coo_mod
+import flagsparse_public_b200.sparse_operations.spmv_csr as spmv_mod
+from flagsparse_public_b200 import _native as nat
+from flagsparse_public_b200 import _plan
+from tests.conftest import load_golden
+
+
+def test_transpose_structure_matches_reference():
+    g = load_golden("transpose_c64")
+    td, ti, tp, tshape = spmv_mod._transpose_csr_for_spmv(g["data"], g["indices"], g["indptr"], g["shape"])
+    assert tshape == tuple(g["t_shape"])
+    assert ti.dtype == g["t_indices"].dtype and tp.dtype == g["t_indptr"].dtype
+    assert torch.equal(ti, g["t_indices"])
+    assert torch.equal(tp, g["t_indptr"])
+    assert torch.equal(td, g["t_data"])
+
+
+def test_coo_to_csr_matches_reference():
+    g = load_golden("coo_to_csr")
+    d, i, p = spmv_mod.coo_to_csr_for_spmv(g["data"], g["row"], g["col"], g["shape"])
+    assert torch.equal(d, g["out_data"]) and torch.equal(i, g["out_indices"]) and torch.equal(p, g["out_indptr"])
+    assert i.dtype == torch.int32 and p.dtype == torch.int64
+
+
+@pytest.mark.parametrize("name", ["spmv_coo_seg_f32", "spmv_coo_seg_c128"])
+def test_coo_sort_and_row_runs_match_reference(name):
+    g = load_golden(name)
+    d, r, c = spmv_coo_mod._sort_coo_lex_inplace(g["data"], g["row"], g["col"], g["shape"][1])
+    assert torch.equal(d, g["sorted_data"]) and torch.equal(r, g["sorted_row"]) and torch.equal(c, g["sorted_col"])
+    seg = spmv_coo_mod._seg_starts_from_sorted_rows(r, d.numel(), d.device)
+    assert torch.equal(seg, g["seg_starts"]) and seg.dtype == g["seg_starts"].dtype
+
+
+def test_split_metadata_matches_reference_host_loop():
+    g = load_golden("spmm_opt_split_f32")
+    rl = g["indptr"][1:] - g["indptr"][:-1]
+    _buckets, long_rows = spmm_mod._build_spmm_opt_buckets(rl)
+    assert torch.equal(long_rows, g["long_rows"])
+    rows, starts, ends, rpp = spmm_mod._build_spmm_opt_split_metadata(g["indptr"], long_rows, 256)
+    assert torch.equal(rows, g["part_rows"]) and rows.dtype == g["part_rows"].dtype
+    assert torch.equal(starts, g["part_starts"]) and torch.equal(ends, g["part_ends"])
+    assert torch.equal(rpp, g["row_part_ptr"])
+
+
+def test_coalesce_matches_reference():
+    g = load_golden("spmm_coo_f32")
+    d, r, c = spmm_coo_mod._coalesce_coo_entries(g["data"], g["row"], g["col"], g["shape"])
+    assert torch.equal(r, g["coalesced_row"]) and torch.equal(c, g["coalesced_col"])
+    assert torch.equal(d, g["coalesced_data"])
+
+
+def _cpu_csr():
+    data = torch.tensor([1.0, 2.0, 3.0])
+    indices = torch.tensor([0, 1, 1], dtype=torch.int32)
+    indptr = torch.tensor([0, 2, 3], dtype=torch.int64)
+    return data, indices, indptr
+
+
+def test_validation_errors_before_device_work():
+    data, indices, indptr = _cpu_csr()
+    with pytest.raises(ValueError, match="must be CUDA tensors"):
+        spmv_mod.prepare_spmv_csr(data, indices, indptr, (2, 2))
+    with pytest.raises(ValueError, match="indptr length"):
+        spmv_mod.prepare_spmv_csr(data, indices, indptr[:-1], (2, 2))
+    with pytest.raises(TypeError, match="must all be torch.Tensor"):
+        spmv_mod.prepare_spmv_csr([1.0], indices, indptr, (2, 2))
+    with pytest.raises(ValueError, match="index_fallback_policy"):
+        spmv_mod.prepare_spmv_csr(data, indices, indptr, (2, 2), index_fallback_policy="bad")
+    with pytest.raises(ValueError, match="op must be one of"):
+        spmv_mod.flagsparse_spmv_csr(data, indices, indptr, data[:2], (2, 2), op="bogus")
+    with pytest.raises(ValueError, match="conflicts with op"):
+        spmv_mod.flagsparse_spmv_csr(data, indices, indptr, data[:2], (2, 2), op="non", transpose=True)
+    with pytest.raises(ValueError, match="must be CUDA tensors"):
+        spmm_mod.flagsparse_spmm_csr(data, indices, indptr, torch.randn(2, 4), (2, 2))
+    with pytest.raises(ValueError, match="shape must be a 2-tuple"):
+        spmm_mod.flagsparse_spmm_csr(data, indices, indptr, torch.randn(2, 4), (2,))
+    with pytest.raises(ValueError, match="block_n must be positive"):
+        spmm_mod.flagsparse_spmm_csr(data, indices, indptr, torch.randn(2, 4), (2, 2), block_n=0)
+    with pytest.raises(ValueError, match="CUDA tensors"):
+        spmm_coo_mod.flagsparse_spmm_coo(data, indices, indices, torch.randn(2, 4), (2, 2))
+    with pytest.raises(ValueError, match="CUDA tensors"):
+        spmv_coo_mod.prepare_spmv_coo(data, indices, indices, (2, 2))
+
+
+def test_op_normalisation():
+    assert spmv_mod._normalize_spmv_op(None, transpose=True) == spmv_mod.SPMV_OP_TRANS
+    assert spmv_mod._normalize_spmv_op("conj") == spmv_mod.SPMV_OP_CONJ_TRANS
+    assert spmv_mod._normalize_spmv_op(1) == spmv_mod.SPMV_OP_TRANS
+    assert spmv_coo_mod._normalize_spmv_coo_op(" NON ") == 0
+    with pytest.raises(ValueError):
+        spmv_coo_mod._normalize_spmv_coo_op(3)
+
+
+def _prepared_cpu(index_dtype, policy="auto"):
+    data, indices, indptr = _cpu_csr()
+    return spmv_mod.PreparedCsrSpmv(
+        data=data, kernel_indices=indices.to(index_dtype), kernel_indptr=indptr.to(index_dtype), shape=(2, 2),
+        n_rows=2, n_cols=2, block_nnz=256, max_segments=1, max_row_nnz=2, opt_buckets=[],
+        index_fallback_policy=policy)
+
+
+def test_int64_failure_falls_back_to_int32(monkeypatch):
+    seen = []
+
+    def fake_run(prepared, x, use_opt=False):
+        seen.append(prepared.kernel_indices.dtype)
+        if prepared.kernel_indices.dtype == torch.int64:
+            raise RuntimeError("forced int64 launch failure")
+        return torch.zeros(prepared.n_rows)
+
+    monkeypatch.setattr(spmv_mod, "_run_spmv_prepared", fake_run)
+    y = spmv_mod._run_spmv_prepared_with_fallback(_prepared_cpu(torch.int64), torch.zeros(2))
+    assert seen == [torch.int64, torch.int32] and y.numel() == 2
+
+
+def test_strict_policy_reraises(monkeypatch):
+    def fake_run(prepared, x, use_opt=False):
+        raise RuntimeError("forced int64 launch failure")
+
+    monkeypatch.setattr(spmv_mod, "_run_spmv_prepared", fake_run)
+    with pytest.raises(RuntimeError, match="forced int64 launch failure"):
+        spmv_mod._run_spmv_prepared_with_fallback(_prepared_cpu(torch.int64, "strict"), torch.zeros(2))
+
+
+def test_fallback_refused_when_index_exceeds_int32(monkeypatch):
+    limit = spmv_mod._INDEX_LIMIT_INT32
+    prepared = spmv_mod.PreparedCsrSpmv(
+        data=torch.ones(1), kernel_indices=torch.tensor([limit + 1], dtype=torch.int64),
+        kernel_indptr=torch.tensor([0, 1], dtype=torch.int64), shape=(1, limit + 2), n_rows=1, n_cols=limit + 2,
+        block_nnz=256, max_segments=1, max_row_nnz=1, opt_buckets=[], transpose=False,
+        index_fallback_policy="auto")
+
+    def fail_launch(_prepared, _x, use_opt=False):
+        raise RuntimeError("forced native int64 failure")
+
+    monkeypatch.setattr(spmv_mod, "_run_spmv_prepared", fail_launch)
+    with pytest.raises(RuntimeError, match="int32 fallback is unsafe"):
+        spmv_mod._run_spmv_prepared_with_fallback(prepared, torch.empty(0), use_opt=False)
+
+
+def test_coo_fallback_policy(monkeypatch):
+    data = torch.tensor([1.0, 2.0])
+    row = torch.tensor([0, 1], dtype=torch.int64)
+    col = torch.tensor([1, 0], dtype=torch.int64)
+    p = spmv_coo_mod.PreparedCoo(data, row, col, (2, 2), seg_starts=torch.tensor([0, 1, 2]))
+    calls = []
+
+    def fake(prepared, x, block_size, num_warps, block_inner):
+        calls.append(prepared.row.dtype)
+        if prepared.row.dtype == torch.int64:
+            raise RuntimeError("forced")
+        return torch.zeros(2)
+
+    monkeypatch.setattr(spmv_coo_mod, "_triton_spmv_coo_kernel", fake)
+    spmv_coo_mod._run_spmv_coo_prepared_with_fallback(p, torch.zeros(2), 256, 4, 128)
+    assert calls == [torch.int64, torch.int32]
+
+
+def test_default_plans():
+    flat = _plan.MatrixStats(16384, 16384, 262144, 35, 16.0, 4.0, 0)
+    p = _plan.default_spmv_plan(flat, torch.float32)
+    assert p.algo == nat.ALGO_ROWS and p.lanes == 4
+    skew = _plan.MatrixStats(262144, 262144, 3_100_000, 7200, 11.9, 80.0, 10)
+    assert _plan.default_spmv_plan(skew, torch.float32).algo == nat.ALGO_MERGE
+    mm = _plan.default_spmm_plan(skew, 64, torch.float32)
+    assert mm.algo == nat.ALGO_MERGE and mm.items_per_unit > 0
+    capped = _plan.default_spmv_plan(skew, torch.float32, row_cap=32)
+    assert capped.algo == nat.ALGO_ROWS and capped.row_cap == 32

@@ -1,0 +1,58 @@
+"""The C-ABI library loads on a machine without a GPU and exports every entry
+point include/flagsparse_b200.h declares (no kernel is launched here)."""
+
+import ctypes
+import os
+import re
+
+from flagsparse_public_b200 import _native as nat
+from tests.conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "flagsparse_b200.h")
+
+
+def declared_in_header():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(fsb_[a-z0-9_]+)\s*\(", text)))
+
+
+def test_header_declarations_are_bound():
+    declared = declared_in_header()
+    assert declared, "no declarations parsed"
+    assert declared == nat.declared_symbols()
+
+
+def test_library_exports_every_declared_symbol():
+    lib = ctypes.CDLL(nat.LIB_PATH)
+    for name in declared_in_header():
+        assert hasattr(lib, name), name
+
+
+def test_abi_version_and_status_strings():
+    lib = nat.library()
+    assert lib.fsb_abi_version() == 1
+    assert lib.fsb_status_string(0) == b"ok"
+    assert b"workspace" in lib.fsb_status_string(nat.FSB_ERR_WORKSPACE)
+
+
+def test_workspace_query_is_host_only():
+    lib = nat.library()
+    m = nat.FsbCsr()
+    m.value_dtype, m.index_dtype, m.ptr_dtype = nat.FSB_F32, nat.FSB_I32, nat.FSB_I64
+    m.n_rows, m.n_cols, m.nnz = 1000, 1000, 5000
+    rows = nat.make_plan(nat.ALGO_ROWS, lanes=4)
+    assert lib.fsb_workspace_bytes(0, m, 1, nat.ACC_NATIVE, nat.FSB_F32, rows) == 0
+    merge = nat.make_plan(nat.ALGO_MERGE, items_per_unit=1024, n_units=6)
+    # carry_row (int64) + carry and head partials per unit, 256-byte aligned
+    assert lib.fsb_workspace_bytes(0, m, 1, nat.ACC_WIDE, nat.FSB_F32, merge) == 3 * 256
+    assert lib.fsb_workspace_bytes(1, m, 64, nat.ACC_NATIVE, nat.FSB_F32, merge) == 256 + 2 * 1536
+
+
+def test_invalid_arguments_rejected_without_launch():
+    lib = nat.library()
+    rc = lib.fsb_spmv_csr(None, None, None, nat.FSB_F32, 0, None, None, 0, None)
+    assert rc == nat.FSB_ERR_INVALID
+    assert b"null" in lib.fsb_last_error()
+    rc = lib.fsb_merge_partition(None, nat.FSB_I64, 10, 10, 128, 0, None, 1, None)
+    assert rc == nat.FSB_ERR_INVALID
