@@ -53,6 +53,9 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + timed device steps (for a profiler launch list)")
+    ap.add_argument("--plan", default=None,
+                    help="force the chosen-form plan: rows:<lanes>[:<n_tile>] | merge:<items>:<snap> | "
+                         "flat|gather:<items>:<snap>[:<n_tile>]")
     return ap.parse_args(argv)
 
 
@@ -241,6 +244,9 @@ class SpmmPowerlaw:
 
         return _spmm_plan_for(self.prepared, "opt", self.n_dense).describe()
 
+    def force_plan(self, plan):
+        self.prepared._plans[("opt", self.n_dense)] = plan
+
     # end to end through the public API from pinned host memory
     def host_inputs(self):
         data, indices, indptr = self.A
@@ -349,6 +355,10 @@ class SpmvPoisson:
 
         return _spmv_plan(self.prepared, "opt").describe()
 
+    def force_plan(self, plan):
+        self.prepared._plans[("opt", 0)] = plan
+        self.graph = self._capture(use_opt=True)
+
     def host_inputs(self):
         data, indices, indptr = self.A
         self.h = [t.cpu().pin_memory() for t in (data, indices, indptr, self.x)]
@@ -456,6 +466,19 @@ def run_reference(args):
     return 0
 
 
+def parse_plan(text):
+    from flagsparse_public_b200 import _native as nat
+    from flagsparse_public_b200 import _plan
+
+    parts = text.split(":")
+    kind, nums = parts[0], [int(v) for v in parts[1:]]
+    if kind == "rows":
+        return _plan.KernelPlan(nat.ALGO_ROWS, lanes=nums[0], n_tile=nums[1] if len(nums) > 1 else 0)
+    algo = {"merge": nat.ALGO_MERGE, "flat": nat.ALGO_FLAT, "gather": nat.ALGO_GATHER}[kind]
+    return _plan.KernelPlan(algo, items_per_unit=nums[0], snap=nums[1] if len(nums) > 1 else 0,
+                            n_tile=nums[2] if len(nums) > 2 else 0)
+
+
 def run_ours(args):
     from flagsparse_public_b200 import _plan
 
@@ -465,6 +488,8 @@ def run_ours(args):
     device = torch.device("cuda", local_rank)
     wl = WORKLOADS[args.workload]()
     wl.build(device)
+    if args.plan:
+        wl.force_plan(parse_plan(args.plan))
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
 
     for _ in range(args.warmup):
@@ -478,7 +503,7 @@ def run_ours(args):
     launches = _plan.LAUNCHES["count"] - launches0
     if graph_launches:
         # graph replays launch the captured kernels without passing through Python
-        launches = args.steps * graph_launches * (2 if wl.plan_desc()["kind"] == "merge_path" else 1)
+        launches = args.steps * graph_launches * (1 if wl.plan_desc()["kind"].endswith("rows") else 2)
     barrier(world)
     total_ms = max_over_ranks(sum(times), world)
     ms_step = total_ms / args.steps

@@ -25,7 +25,7 @@ FSB_ERR_LIMIT = -6
 
 FSB_F16, FSB_BF16, FSB_F32, FSB_F64, FSB_C64, FSB_C128, FSB_I32, FSB_I64 = range(8)
 ACC_NATIVE, ACC_WIDE, ACC_COMP = 0, 1, 2
-ALGO_ROWS, ALGO_MERGE = 0, 1
+ALGO_ROWS, ALGO_MERGE, ALGO_FLAT, ALGO_GATHER = 0, 1, 2, 3
 
 _DTYPE_CODES = {
     torch.float16: FSB_F16,
@@ -75,6 +75,8 @@ _SIGNATURES = {
     "fsb_abi_version": (ctypes.c_int, []),
     "fsb_status_string": (ctypes.c_char_p, [ctypes.c_int]),
     "fsb_last_error": (ctypes.c_char_p, []),
+    "fsb_device_error": (ctypes.c_int, [ctypes.POINTER(ctypes.c_int), ctypes.c_int]),
+    "fsb_selftest_wait_timeout": (ctypes.c_int, [ctypes.c_int64, ctypes.c_void_p]),
     "fsb_workspace_bytes": (
         ctypes.c_int64,
         [ctypes.c_int, ctypes.POINTER(FsbCsr), ctypes.c_int64, ctypes.c_int, ctypes.c_int, ctypes.POINTER(FsbPlan)],
@@ -135,6 +137,13 @@ def library():
             fn.argtypes = args
         _lib = lib
     return _lib
+
+
+def device_error(reset=True):
+    """Sticky device error word of the mbarrier-waiting kernels (synchronises)."""
+    v = ctypes.c_int(0)
+    check(library().fsb_device_error(ctypes.byref(v), int(bool(reset))), "fsb_device_error")
+    return v.value
 
 
 def declared_symbols():

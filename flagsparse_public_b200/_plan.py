@@ -24,7 +24,7 @@ LAUNCHES = {"count": 0}
 
 
 def _kernels_per_call(plan):
-    return 2 if plan.algo == nat.ALGO_MERGE else 1
+    return 1 if plan.algo == nat.ALGO_ROWS else 2
 
 
 class MatrixStats:
@@ -63,9 +63,10 @@ class KernelPlan:
     """One launch configuration of fsb_spmv_csr / fsb_spmm_csr."""
 
     __slots__ = ("algo", "lanes", "items_per_unit", "n_tile", "snap", "coords", "n_units", "row_cap",
-                 "comp_threshold")
+                 "comp_threshold", "fallback_ok")
 
-    def __init__(self, algo, lanes=32, items_per_unit=0, n_tile=0, snap=0, row_cap=0, comp_threshold=0):
+    def __init__(self, algo, lanes=32, items_per_unit=0, n_tile=0, snap=0, row_cap=0, comp_threshold=0,
+                 fallback_ok=False):
         self.algo = int(algo)
         self.lanes = int(lanes)
         self.items_per_unit = int(items_per_unit)
@@ -75,6 +76,14 @@ class KernelPlan:
         self.n_units = 0
         self.row_cap = int(row_cap)
         self.comp_threshold = int(comp_threshold)
+        self.fallback_ok = bool(fallback_ok)
+
+    def as_flat(self):
+        """The register-staged flat plan over the same merge-path units."""
+        p = KernelPlan(nat.ALGO_FLAT, items_per_unit=self.items_per_unit, n_tile=self.n_tile, snap=self.snap,
+                       row_cap=self.row_cap, comp_threshold=self.comp_threshold)
+        p.coords, p.n_units = self.coords, self.n_units
+        return p
 
     def key(self):
         return (self.algo, self.lanes, self.items_per_unit, self.n_tile, self.snap)
@@ -83,17 +92,19 @@ class KernelPlan:
         if self.algo == nat.ALGO_ROWS:
             kind = "warp_rows" if self.lanes == 32 else "vector_rows"
             return {"kind": kind, "lanes": self.lanes, "n_tile": self.n_tile}
-        return {"kind": "merge_path", "items_per_unit": self.items_per_unit, "n_tile": self.n_tile,
+        kind = {nat.ALGO_MERGE: "merge_path", nat.ALGO_FLAT: "merge_path_flat",
+                nat.ALGO_GATHER: "merge_path_tma_gather"}[self.algo]
+        return {"kind": kind, "items_per_unit": self.items_per_unit, "n_tile": self.n_tile,
                 "snap": self.snap, "n_units": self.n_units}
 
     def copy(self):
         p = KernelPlan(self.algo, self.lanes, self.items_per_unit, self.n_tile, self.snap, self.row_cap,
-                       self.comp_threshold)
+                       self.comp_threshold, self.fallback_ok)
         return p
 
     def ensure_coords(self, row_ptr, n_rows, nnz):
         """Compute (once) the merge-path unit coordinates on the device."""
-        if self.algo != nat.ALGO_MERGE or self.coords is not None:
+        if self.algo == nat.ALGO_ROWS or self.coords is not None:
             return
         n_units = -(-(int(n_rows) + int(nnz)) // self.items_per_unit) if (n_rows + nnz) > 0 else 0
         coords = torch.empty((n_units + 1) * 2, dtype=torch.int64, device=row_ptr.device)
@@ -141,6 +152,14 @@ def default_spmm_plan(stats, n_dense, dtype, row_cap=0):
     skewed rows; warp per row for medium rows; vector per row for short rows."""
     if row_cap > 0 or stats.n_rows == 0:
         return KernelPlan(nat.ALGO_ROWS, lanes=32, row_cap=row_cap)
+    elem = torch.empty((), dtype=dtype).element_size()
+    vw = max(1, 16 // max(elem, 4 if dtype in (torch.float16, torch.bfloat16) else elem))
+    if n_dense >= 8 * vw and (n_dense * elem) % 16 == 0:
+        # TMA bulk gathers of B rows (falls back to the register-staged flat
+        # kernel at run time when B / C rows are not 16-byte aligned)
+        return KernelPlan(nat.ALGO_GATHER, items_per_unit=256, fallback_ok=True)
+    if n_dense >= 8:
+        return KernelPlan(nat.ALGO_FLAT, items_per_unit=256)
     skewed = stats.max_row > 8 * max(stats.mean_row, 1.0) + 64
     if skewed:
         return KernelPlan(nat.ALGO_MERGE, items_per_unit=128, snap=64)
@@ -174,8 +193,30 @@ def run_spmv(values, col_idx, row_ptr, n_rows, n_cols, x, y, acc_mode, plan, row
     return y
 
 
+def gather_supported(B, C, n_tile=0):
+    """Whether the TMA bulk-gather plan can run on these operands: 16-byte
+    aligned B rows, column tiles and C lane vectors (mirrors the check in
+    fsb_spmm_gather.cu)."""
+    vb, vc = B.element_size(), C.element_size()
+    vw = max(1, 16 // max(vb, vc))
+    n_dense = B.shape[1]
+    target = n_tile if n_tile > 0 else n_dense
+    lpn_log2 = 0
+    while (1 << lpn_log2) * vw < target and lpn_log2 < 5:
+        lpn_log2 += 1
+    tile_bytes = (vw << lpn_log2) * vb
+    multi_tile = n_dense > (vw << lpn_log2)
+    return (lpn_log2 >= 3 and B.data_ptr() % 16 == 0 and (B.stride(0) * vb) % 16 == 0 and (n_dense * vb) % 16 == 0
+            and (not multi_tile or tile_bytes % 16 == 0) and C.data_ptr() % (vw * vc) == 0
+            and C.stride(0) % vw == 0 and n_dense % vw == 0)
+
+
 def run_spmm(values, col_idx, row_ptr, n_rows, n_cols, B, C, acc_mode, plan, row_map=None):
     """C = A B through fsb_spmm_csr (B, C row-major with unit column stride)."""
+    if plan.algo == nat.ALGO_GATHER and not gather_supported(B, C, plan.n_tile):
+        if not plan.fallback_ok:
+            raise ValueError("the TMA gather plan needs 16-byte aligned B and C rows")
+        plan = plan.as_flat()
     plan.ensure_coords(row_ptr, n_rows, values.numel())
     n_dense = int(B.shape[1])
     cm = nat.make_csr(values, col_idx, row_ptr, n_rows, n_cols, row_map)

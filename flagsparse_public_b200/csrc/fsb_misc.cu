@@ -103,7 +103,8 @@ extern "C" const char* fsb_last_error(void) { return fsb_host::g_last_error; }
 extern "C" int64_t fsb_workspace_bytes(int is_spmm, const fsb_csr* A, int64_t n_dense, int acc_mode, int out_dtype,
                                        const fsb_plan* plan) {
     (void)out_dtype;
-    if (!A || !plan || plan->algo != FSB_ALGO_MERGE) return 0;
+    if (!A || !plan) return 0;
+    if (plan->algo != FSB_ALGO_MERGE && plan->algo != FSB_ALGO_FLAT && plan->algo != FSB_ALGO_GATHER) return 0;
     const int ab = acc_size(A->value_dtype, acc_mode);
     if (ab == 0) return 0;
     return merge_scratch_bytes(plan->n_units, is_spmm ? n_dense : 1, ab);

@@ -20,11 +20,10 @@
 // (spmm_csr.py:92-195), the opt bucket kernels (:602-775), the long-row split
 // kernels (:778-919), the alg2 kernels (spmm_csr_opt_alg2.py:338-629) and the
 // COO row-run kernels (spmm_coo.py:135-241).
-#include "fsb_dispatch.cuh"
+#include "fsb_spmm_common.cuh"
 
 namespace fsb {
 
-constexpr int kSpmmThreads = 128;
 constexpr int kSpmmUnroll = 4;
 
 struct Lanes {
@@ -70,20 +69,6 @@ __device__ __forceinline__ void row_segment(const V* __restrict__ val, const I* 
 #pragma unroll
                 for (int w = 0; w < VW; ++w) acc[w] = Acc<V, A>::fma(av[u], bv[u].v[w], acc[w]);
         }
-    }
-}
-
-template <class O, class A, int VW>
-__device__ __forceinline__ void store_row(O* __restrict__ C, int64_t ldc, int64_t out_row, int64_t c0,
-                                          const A (&acc)[VW]) {
-    if constexpr (VW > 1 && (sizeof(O) * VW == 16 || sizeof(O) * VW == 8 || sizeof(O) * VW == 4)) {
-        vec_t<O, VW> o;
-#pragma unroll
-        for (int w = 0; w < VW; ++w) o.v[w] = Out<O, A>::cvt(acc[w]);
-        st_stream<O, VW>(C + out_row * ldc + c0, o);
-    } else {
-#pragma unroll
-        for (int w = 0; w < VW; ++w) C[out_row * ldc + c0 + w] = Out<O, A>::cvt(acc[w]);
     }
 }
 
@@ -200,28 +185,228 @@ k_spmm_merge(const V* __restrict__ val, const I* __restrict__ col, const P* __re
     if (blockIdx.y == 0 && L.lig == 0) carry_row[unit] = open ? r1 : -1;
 }
 
-// One warp per unit: the first unit of each run carrying the same open row
-// folds the run's carries (unit order) and the ending unit's head partial.
-template <class A, class O, class I, class P>
+// ------------------------------------------------------------ flat units ----
+// One warp per (merge-path unit, column tile of LPN * VW columns).  Lane l owns
+// columns [c0, c0 + VW) of the tile (16-byte vectors) and sub-group
+// s = l / LPN takes every NPAR-th nonzero of the unit's stream (NPAR = 32 /
+// LPN), so one warp step advances NPAR nonzeros.  The unit's values and column
+// indices stream through a 32-entry register window (the next window is
+// prefetched), row ends through a second 32-entry window, and kFlatU steps of
+// B rows are gathered before they are accumulated.  When a step crosses the
+// current row's end, the sub-groups' partials meet in a xor butterfly and the
+// row is flushed: to C, or -- for the unit's first row when it began in an
+// earlier unit -- to head_val; the row left open at the unit's end goes to
+// carry_val (folded in by k_spmm_merge_fixup, in unit order).
+constexpr int kFlatU = 4;
+
+template <class V, class A, class O, class I, class P, int VW, bool ADDR32>
 __global__ void __launch_bounds__(kSpmmThreads)
-k_spmm_merge_fixup(const int64_t* __restrict__ carry_row, const A* __restrict__ carry_val,
-                   const A* __restrict__ head_val, int64_t n_units, int64_t n_dense, const P* __restrict__ ptr,
-                   const I* __restrict__ row_map, O* __restrict__ C, int64_t ldc) {
-    const int64_t t = (int64_t)blockIdx.x * (kSpmmThreads / 32) + (threadIdx.x >> 5);
+k_spmm_flat(const V* __restrict__ val, const I* __restrict__ col, const P* __restrict__ ptr,
+            const I* __restrict__ row_map, const V* __restrict__ B, int64_t ldb, O* __restrict__ C, int64_t ldc,
+            int64_t n_rows, int64_t n_dense, int lpn_log2, const int64_t* __restrict__ coords, int64_t n_units,
+            int64_t* __restrict__ carry_row, A* __restrict__ carry_val, A* __restrict__ head_val) {
     const int lane = threadIdx.x & 31;
-    if (t >= n_units) return;
-    const int64_t r = carry_row[t];
-    if (r < 0) return;
-    if (t > 0 && carry_row[t - 1] == r) return;
-    int64_t u_end = t + 1;
-    while (u_end < n_units && carry_row[u_end] == r) ++u_end;
-    const int64_t out_row = row_map ? idx(row_map[idx(ptr[r])]) : r;
-    for (int64_t c = lane; c < n_dense; c += 32) {
-        A sum = carry_val[t * n_dense + c];
-        for (int64_t u = t + 1; u < u_end; ++u) sum = acc_add(sum, carry_val[u * n_dense + c]);
-        if (u_end < n_units) sum = acc_add(sum, head_val[u_end * n_dense + c]);
-        C[out_row * ldc + c] = Out<O, A>::cvt(sum);
+    const int64_t unit = (int64_t)blockIdx.x * (kSpmmThreads / 32) + (threadIdx.x >> 5);
+    if (unit >= n_units) return;
+    const unsigned full = 0xffffffffu;
+    const int LPN = 1 << lpn_log2;
+    const int NPAR = 32 >> lpn_log2;
+    const int sub = lane >> lpn_log2;
+    const int U = NPAR * kFlatU <= 32 ? kFlatU : 32 / NPAR;  // steps per batch, batch stays in one window
+    const int64_t c0 = (int64_t)blockIdx.y * (LPN * VW) + (int64_t)(lane & (LPN - 1)) * VW;
+    const bool col_ok = c0 < n_dense;
+
+    const int64_t r0 = coords[2 * unit], k0 = coords[2 * unit + 1];
+    const int64_t r1 = coords[2 * unit + 2], k1 = coords[2 * unit + 3];
+    const int64_t last_row = r1 < n_rows ? r1 : r1 - 1;  // last row this unit touches
+    constexpr int64_t kNoEnd = INT64_MAX;
+
+    // Row-end window: lane l holds ptr[rb + l + 1] (rows rb .. rb + 31).
+    int64_t rb = r0;
+    int64_t e_win = (rb + lane <= last_row) ? idx(ptr[rb + lane + 1]) : kNoEnd;
+    int64_t row = r0;
+    int64_t row_start = (r0 < n_rows) ? idx(ptr[r0]) : k0;
+    const bool continued = (r0 < n_rows) && (k0 > row_start);
+    int64_t row_end = (r0 <= last_row) ? __shfl_sync(full, e_win, 0) : kNoEnd;
+
+    // Nonzero windows: lane l holds entry kb + l (current) and kb + 32 + l (next).
+    int64_t kb = k0;
+    V v_cur = vzero<V>(), v_nxt = vzero<V>();
+    I c_cur = 0, c_nxt = 0;
+    if (kb + lane < k1) { v_cur = ld_stream1(val + kb + lane); c_cur = ld_stream1(col + kb + lane); }
+    if (kb + 32 + lane < k1) { v_nxt = ld_stream1(val + kb + 32 + lane); c_nxt = ld_stream1(col + kb + 32 + lane); }
+
+    A acc[VW];
+    zero_acc<A, VW>(acc);
+
+    auto reduce = [&]() {
+#pragma unroll
+        for (int w = 0; w < VW; ++w) acc[w] = segment_reduce(full, acc[w], LPN, 32);
+    };
+    auto flush = [&](int64_t r, int64_t r_start) {
+        reduce();
+        if (sub == 0 && col_ok) {
+            if (r == r0 && continued) {
+                A* dst = head_val + unit * n_dense + c0;
+#pragma unroll
+                for (int w = 0; w < VW; ++w) dst[w] = acc[w];
+            } else {
+                const int64_t out_row = row_map ? idx(row_map[r_start]) : r;
+                store_row<O, A, VW>(C, ldc, out_row, c0, acc);
+            }
+        }
+        zero_acc<A, VW>(acc);
+    };
+    auto advance = [&]() {
+        ++row;
+        row_start = row_end;
+        if (row > last_row) return kNoEnd;
+        if (row - rb >= 32) {
+            rb += 32;
+            e_win = (rb + lane <= last_row) ? idx(ptr[rb + lane + 1]) : kNoEnd;
+        }
+        return __shfl_sync(full, e_win, (int)(row - rb));
+    };
+
+    int64_t k = k0;
+    while (k < k1) {
+        // a batch covers U steps of NPAR nonzeros, never past the window or k1
+        int64_t lim = k1 - k;
+        if (kb + 32 - k < lim) lim = kb + 32 - k;
+        const int n_here = lim < (int64_t)(NPAR * U) ? (int)lim : NPAR * U;
+        const int base = (int)(k - kb);
+        vec_t<V, VW> bv[kFlatU];
+        V av[kFlatU];
+#pragma unroll
+        for (int u = 0; u < kFlatU; ++u) {
+            if (u < U) {
+                const int j = u * NPAR + sub;
+                const int src = (base + j) & 31;
+                av[u] = shfl_idx(full, v_cur, src, 32);
+                const I cc = shfl_idx(full, c_cur, src, 32);
+                if (j < n_here && col_ok) {
+                    const V* bp = ADDR32 ? B + (int32_t)((int32_t)cc * (int32_t)ldb + (int32_t)c0)
+                                         : B + idx(cc) * ldb + c0;
+                    bv[u] = ld_ro<V, VW>(bp);
+                } else {
+#pragma unroll
+                    for (int w = 0; w < VW; ++w) bv[u].v[w] = vzero<V>();
+                }
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < kFlatU; ++u) {
+            if (u < U && u * NPAR < n_here) {
+                const int64_t step = k + u * NPAR;
+                const int64_t my_k = step + sub;
+                const int64_t step_last = (step + NPAR < k1 ? step + NPAR : k1) - 1;
+                bool done = my_k >= k1;
+                while (step_last >= row_end) {
+                    if (!done && my_k < row_end) {
+#pragma unroll
+                        for (int w = 0; w < VW; ++w) acc[w] = Acc<V, A>::fma(av[u], bv[u].v[w], acc[w]);
+                        done = true;
+                    }
+                    flush(row, row_start);
+                    row_end = advance();
+                }
+                if (!done) {
+#pragma unroll
+                    for (int w = 0; w < VW; ++w) acc[w] = Acc<V, A>::fma(av[u], bv[u].v[w], acc[w]);
+                }
+            }
+        }
+        k += n_here;
+        if (k == kb + 32) {
+            kb += 32;
+            v_cur = v_nxt;
+            c_cur = c_nxt;
+            if (kb + 32 + lane < k1) {
+                v_nxt = ld_stream1(val + kb + 32 + lane);
+                c_nxt = ld_stream1(col + kb + 32 + lane);
+            }
+        }
     }
+    // Rows ending exactly at k1 (and empty rows) still owned by this unit.
+    while (row < r1) {
+        flush(row, row_start);
+        row_end = advance();
+    }
+    bool open = false;
+    if (r1 < n_rows) {
+        const int64_t s1 = row_start > k0 ? row_start : k0;  // row == r1 here
+        open = k1 > s1;
+        if (open) {
+            reduce();
+            if (sub == 0 && col_ok) {
+                A* dst = carry_val + unit * n_dense + c0;
+#pragma unroll
+                for (int w = 0; w < VW; ++w) dst[w] = acc[w];
+            }
+        }
+    }
+    if (blockIdx.y == 0 && lane == 0) carry_row[unit] = open ? r1 : -1;
+}
+
+template <class V, class A, class O, class I, class P>
+int launch_spmm_flat(const fsb_csr* Am, const V* val, const I* col, const P* ptr, const I* rmap, const V* B,
+                     int64_t ldb, int64_t n_dense, O* C, int64_t ldc, const fsb_plan* plan, void* workspace,
+                     int64_t workspace_bytes, cudaStream_t st) {
+    const int64_t n_units = plan->n_units;
+    if (plan->items_per_unit < 1 || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
+        !plan->unit_coords) {
+        fsb_host::set_error("fsb_spmm_csr: flat plan does not match the matrix");
+        return FSB_ERR_INVALID;
+    }
+    if (plan->row_cap > 0) {
+        fsb_host::set_error("fsb_spmm_csr: row_cap needs the rows algorithm");
+        return FSB_ERR_INVALID;
+    }
+    const int64_t need = merge_scratch_bytes(n_units, n_dense, (int)sizeof(A));
+    if (!workspace || workspace_bytes < need) {
+        fsb_host::set_error("fsb_spmm_csr: workspace %lld bytes < %lld", (long long)workspace_bytes, (long long)need);
+        return FSB_ERR_WORKSPACE;
+    }
+    // 16-byte lane vectors when B and C rows allow that alignment; LPN lanes
+    // cover the column tile, NPAR = 32 / LPN nonzeros per warp step.
+    constexpr int kMaxBytes = (int)(sizeof(V) > sizeof(O) ? sizeof(V) : sizeof(O));
+    constexpr int kVW = 16 / kMaxBytes >= 1 ? 16 / kMaxBytes : 1;
+    auto vec_ok = [&](int w) {
+        return w == 1 || (((uintptr_t)B) % (w * sizeof(V)) == 0 && ldb % w == 0 && n_dense % w == 0 &&
+                          ((uintptr_t)C) % (w * sizeof(O)) == 0 && ldc % w == 0);
+    };
+    const int vw = (kVW > 1 && vec_ok(kVW)) ? kVW : 1;
+    const int64_t target = plan->n_tile > 0 ? plan->n_tile : n_dense;
+    int lpn_log2 = 0;
+    while ((1LL << lpn_log2) * vw < target && lpn_log2 < 5) ++lpn_log2;
+    const int64_t col_tiles = ceil_div(n_dense, (int64_t)vw << lpn_log2);
+    const int64_t blocks = ceil_div(n_units, kSpmmThreads / 32);
+    if (col_tiles > 65535 || blocks > 0x7fffffffLL) {
+        fsb_host::set_error("fsb_spmm_csr: flat grid too large");
+        return FSB_ERR_LIMIT;
+    }
+    // 32-bit B offsets when every element of B is addressable that way
+    const bool addr32 = (Am->n_cols * ldb + n_dense) < 0x7fffffffLL;
+    MergeScratch ms = merge_scratch_carve(workspace, n_units, n_dense, (int)sizeof(A));
+    dim3 g((unsigned)blocks, (unsigned)col_tiles);
+    A* cv = static_cast<A*>(ms.carry_val);
+    A* hv = static_cast<A*>(ms.head_val);
+#define FSB_FLAT(W, A32)                                                                                        \
+    k_spmm_flat<V, A, O, I, P, W, A32><<<g, kSpmmThreads, 0, st>>>(val, col, ptr, rmap, B, ldb, C, ldc,        \
+                                                                   Am->n_rows, n_dense, lpn_log2,              \
+                                                                   plan->unit_coords, n_units, ms.carry_row, cv, hv)
+    if (vw == kVW && kVW > 1) {
+        if (addr32) FSB_FLAT(kVW, true); else FSB_FLAT(kVW, false);
+    } else {
+        if (addr32) FSB_FLAT(1, true); else FSB_FLAT(1, false);
+    }
+#undef FSB_FLAT
+    int rc = fsb_host::check_launch("k_spmm_flat");
+    if (rc) return rc;
+    k_spmm_merge_fixup<A, O, I, P><<<(unsigned)blocks, kSpmmThreads, 0, st>>>(
+        ms.carry_row, static_cast<const A*>(ms.carry_val), static_cast<const A*>(ms.head_val), n_units, n_dense, ptr,
+        rmap, C, ldc);
+    return fsb_host::check_launch("k_spmm_merge_fixup");
 }
 
 template <class V, class A, class O, class I, class P, int VW>
@@ -318,6 +503,9 @@ extern "C" int fsb_spmm_csr(const fsb_csr* A, const void* B, int64_t ldb, int64_
         return FSB_ERR_INVALID;
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (plan->algo == FSB_ALGO_GATHER)
+        return spmm_gather_dispatch(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes,
+                                    st);
     return dispatch_vao(A->value_dtype, acc_mode, out_dtype, [&](auto tv, auto ta, auto to) -> int {
         using V = typename decltype(tv)::type;
         using Ac = typename decltype(ta)::type;
@@ -334,6 +522,9 @@ extern "C" int fsb_spmm_csr(const fsb_csr* A, const void* B, int64_t ldb, int64_
                 const I* rmap = static_cast<const I*>(A->row_map);
                 const V* Bv = static_cast<const V*>(B);
                 O* Cv = static_cast<O*>(C);
+                if (plan->algo == FSB_ALGO_FLAT)
+                    return launch_spmm_flat<V, Ac, O, I, P>(A, val, col, ptr, rmap, Bv, ldb, n_dense, Cv, ldc, plan,
+                                                            workspace, workspace_bytes, st);
                 // 16-byte vectors need aligned bases and row strides; the output
                 // vector must be a loadable width too.
                 const bool vec_ok = VW > 1 && aligned16(Bv) && (ldb % VW == 0) && (n_dense % VW == 0) &&

@@ -58,6 +58,11 @@ extern "C" {
 /* ---- algorithms ------------------------------------------------------- */
 #define FSB_ALGO_ROWS   0  /* one group of plan->lanes lanes per row        */
 #define FSB_ALGO_MERGE  1  /* merge-path units over (rows + nonzeros)      */
+#define FSB_ALGO_FLAT   2  /* SpMM: merge-path units, one warp streams the
+                              unit's nonzeros, B rows gathered to registers */
+#define FSB_ALGO_GATHER 3  /* SpMM: merge-path units, B rows gathered into a
+                              shared-memory ring by TMA bulk copies
+                              (cp.async.bulk + mbarrier), several stages deep */
 
 /* A CSR matrix (or a sorted COO matrix seen as row runs).
  * row_ptr has n_rows + 1 entries.  If row_map is non-null, row r of this
@@ -98,6 +103,18 @@ int         fsb_abi_version(void);
 const char* fsb_status_string(int status);
 /* Text of the last error recorded by this thread (launch errors, bad plans). */
 const char* fsb_last_error(void);
+
+/* Sticky device error word of the kernels that wait on mbarriers: 0, or
+ * FSB_ERR_TIMEOUT when a bounded wait gave up (the kernel then drained its
+ * copies in flight and returned).  Synchronises the current device; with
+ * reset != 0 the word is cleared.                                           */
+int fsb_device_error(int* status_out, int reset);
+
+/* Self-test of the bounded waits: one warp waits on an mbarrier that no
+ * thread or copy ever completes; after limit_ns (at most 2 s) it gives up and
+ * records FSB_ERR_TIMEOUT in the device error word, leaving the context
+ * usable.  No FlagSparse counterpart (failure-path test hook).             */
+int fsb_selftest_wait_timeout(int64_t limit_ns, void* stream);
 
 /* Scratch bytes fsb_spmv_csr / fsb_spmm_csr need for this plan (0 for ROWS). */
 int64_t fsb_workspace_bytes(int is_spmm, const fsb_csr* A, int64_t n_dense,

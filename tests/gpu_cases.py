@@ -62,6 +62,10 @@ def spmm_plans():
     plans += [_plan.KernelPlan(nat.ALGO_ROWS, lanes=32, n_tile=8)]
     plans += [_plan.KernelPlan(nat.ALGO_MERGE, items_per_unit=ipu, snap=snap)
               for ipu, snap in ((32, 0), (64, 16), (128, 64), (512, 0))]
+    plans += [_plan.KernelPlan(nat.ALGO_FLAT, items_per_unit=ipu, snap=snap, n_tile=nt)
+              for ipu, snap, nt in ((16, 0, 0), (100, 0, 0), (256, 128, 0), (1024, 0, 0), (128, 64, 32))]
+    plans += [_plan.KernelPlan(nat.ALGO_GATHER, items_per_unit=ipu, snap=snap, n_tile=nt)
+              for ipu, snap, nt in ((16, 0, 0), (100, 0, 0), (256, 128, 0), (2048, 0, 0), (128, 64, 32))]
     return plans
 
 

@@ -26,8 +26,21 @@ REL_BOUND = {
 }
 
 
+# Half the spacing of the subnormal numbers of each result type: rounding a
+# result into the subnormal range errs by up to this much in absolute terms,
+# which no relative bound covers.
+SUBNORMAL_HALF_SPACING = {
+    torch.float16: 2.0 ** -25,
+    torch.bfloat16: 2.0 ** -134,
+    torch.float32: 2.0 ** -150,
+}
+
+
 def scaled_error(actual, exact, mag):
-    """Max over entries of |actual - exact| / max(mag, tiny) (all on CPU, float64)."""
+    """Max over entries of |actual - exact| / max(mag, tiny) (all on CPU, float64).
+
+    For half-precision results the subnormal rounding floor is subtracted first.
+    """
     a = actual.detach().cpu()
     e = exact.detach().cpu()
     if a.numel() == 0:
@@ -36,6 +49,9 @@ def scaled_error(actual, exact, mag):
         diff = (a.to(torch.complex128) - e.to(torch.complex128)).abs()
     else:
         diff = (a.to(torch.float64) - e.to(torch.float64)).abs()
+        floor = SUBNORMAL_HALF_SPACING.get(a.dtype, 0.0)
+        if floor:
+            diff = (diff - floor).clamp(min=0.0)
     denom = mag.detach().cpu().to(torch.float64).clamp(min=1e-300)
     err = diff / denom
     # rows whose magnitude is zero must be exactly zero

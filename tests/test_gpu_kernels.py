@@ -159,6 +159,8 @@ def test_spmm_all_plans(pattern, n_dense, mode):
     Bd = B.to(DEV)
     for plan in spmm_plans():
         C = torch.full((n_rows, n_dense), float("nan"), dtype=out_dtype, device=DEV)
+        if plan.algo == nat.ALGO_GATHER and not _plan.gather_supported(Bd, C, plan.n_tile):
+            continue
         _plan.run_spmm(*d, n_rows, n_cols, Bd, C, acc, plan)
         err = scaled_error(C, exact, mag)
         assert err <= bound, (plan.describe(), err)
@@ -173,7 +175,9 @@ def test_spmm_strided_output_and_operand():
     Cw = torch.zeros((n_rows, 72), device=DEV)
     C = Cw[:, :64]
     lib = nat.library()
-    cm = nat.make_csr(data.to(DEV), indices.to(DEV), indptr.to(DEV), n_rows, n_cols)
+    # the struct holds raw pointers: keep the device tensors alive across the call
+    d_data, d_idx, d_ptr = data.to(DEV), indices.to(DEV), indptr.to(DEV)
+    cm = nat.make_csr(d_data, d_idx, d_ptr, n_rows, n_cols)
     Bd = Bw.to(DEV)
     cp = _plan.KernelPlan(nat.ALGO_ROWS, lanes=32).c_plan()
     rc = lib.fsb_spmm_csr(cm, nat.ptr(Bd), 80, 64, nat.ptr(Cw), 72, nat.FSB_F32, nat.ACC_WIDE, cp, None, 0,
@@ -207,3 +211,32 @@ def test_merge_partition_kernel_matches_oracle():
         plan.ensure_coords(indptr.to(DEV), n_rows, nnz)
         ref = orc.merge_partition(indptr, n_rows, nnz, items, snap)
         assert torch.equal(plan.coords.cpu(), ref)
+
+
+def test_bounded_wait_times_out_and_context_survives():
+    """A wait on an mbarrier nothing completes gives up, records a status, and
+    the device keeps working (no trap, no hang)."""
+    lib = nat.library()
+    assert nat.device_error(reset=True) in (0, nat.FSB_ERR_TIMEOUT)
+    rc = lib.fsb_selftest_wait_timeout(20_000_000, nat.stream_handle(torch.device(DEV)))  # 20 ms
+    nat.check(rc, "fsb_selftest_wait_timeout")
+    torch.cuda.synchronize()
+    assert nat.device_error(reset=True) == nat.FSB_ERR_TIMEOUT
+    assert nat.device_error(reset=False) == 0
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths([5, 0, 40, 3], 300, seed=31)
+    B = dense((n_cols, 64), 32, torch.float32)
+    exact, mag = orc.spmm_csr_exact(data, indices, indptr, B)
+    C = torch.empty((n_rows, 64), device=DEV)
+    _plan.run_spmm(data.to(DEV), indices.to(DEV), indptr.to(DEV), n_rows, n_cols, B.to(DEV), C, nat.ACC_WIDE,
+                   _plan.KernelPlan(nat.ALGO_GATHER, items_per_unit=16))
+    assert scaled_error(C, exact, mag) <= 1e-5
+    assert nat.device_error(reset=False) == 0
+
+
+def test_gather_plan_rejects_unaligned_operands():
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths([5, 7], 50, seed=33)
+    B = dense((n_cols, 6), 34, torch.float32).to(DEV)
+    C = torch.empty((n_rows, 6), device=DEV)
+    with pytest.raises(ValueError, match="16-byte aligned"):
+        _plan.run_spmm(data.to(DEV), indices.to(DEV), indptr.to(DEV), n_rows, n_cols, B, C, nat.ACC_NATIVE,
+                       _plan.KernelPlan(nat.ALGO_GATHER, items_per_unit=16))

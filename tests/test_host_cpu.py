@@ -176,6 +176,8 @@ def test_default_plans():
     skew = _plan.MatrixStats(262144, 262144, 3_100_000, 7200, 11.9, 80.0, 10)
     assert _plan.default_spmv_plan(skew, torch.float32).algo == nat.ALGO_MERGE
     mm = _plan.default_spmm_plan(skew, 64, torch.float32)
-    assert mm.algo == nat.ALGO_MERGE and mm.items_per_unit > 0
+    assert mm.algo == nat.ALGO_GATHER and mm.items_per_unit > 0 and mm.fallback_ok
+    assert mm.as_flat().algo == nat.ALGO_FLAT
+    assert _plan.default_spmm_plan(skew, 4, torch.float32).algo == nat.ALGO_MERGE
     capped = _plan.default_spmv_plan(skew, torch.float32, row_cap=32)
     assert capped.algo == nat.ALGO_ROWS and capped.row_cap == 32
