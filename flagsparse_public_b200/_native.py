@@ -91,6 +91,11 @@ _SIGNATURES = {
         [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
          ctypes.POINTER(FsbPlan), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
     ),
+    "fsb_spmv_csr_noalloc": (
+        ctypes.c_int,
+        [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int32,
+         ctypes.c_void_p],
+    ),
     "fsb_spmm_csr": (
         ctypes.c_int,
         [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,

@@ -16,7 +16,9 @@
 // FlagSparse computes the same products in _spmv_csr_real_kernel
 // (spmv_csr.py:158-184), _spmv_csr_complex_kernel (:187-219), the CSR-vector
 // bucket kernels (:225-343) and the COO row-run kernels (spmv_coo.py:131-226).
-#include "fsb_dispatch.cuh"
+#include <mutex>
+
+#include "fsb_partition.cuh"
 
 namespace fsb {
 
@@ -327,6 +329,129 @@ extern "C" int fsb_spmv_csr(const fsb_csr* A, const void* x, void* y, int out_dt
                     ms.carry_row, static_cast<const Ac*>(ms.carry_val), static_cast<const Ac*>(ms.head_val),
                     n_units, ptr, rmap, yv);
                 return fsb_host::check_launch("k_spmv_merge_fixup");
+            });
+        });
+    });
+}
+
+// --------------------------------------------------- allocation-free SpMV ----
+// fsb_spmv_csr_noalloc: the merge-path SpMV for callers that cannot allocate
+// device memory -- a C program or plug-in that receives device pointers from
+// a host framework owning all device memory, or a latency-critical loop in
+// which cudaMalloc's implicit device-wide synchronisation is not acceptable.
+// The caller still passes the matrix, x and y; the scratch this algorithm
+// needs (merge-path tile coordinates and per-tile carries) lives in the
+// file-scope device array below, of a fixed size, held by every GPU that loads
+// this library until the process exits.
+//
+// Limit: at most kNoAllocMaxTiles merge-path tiles, i.e.
+// n_rows + nnz <= kNoAllocMaxTiles * items_per_unit (16384 tiles: 16.7 M path
+// items at 1024 items per tile); larger matrices are rejected with
+// FSB_ERR_LIMIT.  Every call on a device shares the one array: two calls whose
+// kernels overlap on the GPU (for example on two streams) race on it, so
+// callers must order such calls.  Nothing in the array has to start at zero:
+// each call writes the coordinates and every tile's carry slot before they
+// are read.  The first call on a device resolves the array's device address
+// (cudaGetSymbolAddress) with that device current; that first call should
+// come before any stream capture.
+constexpr int64_t kNoAllocMaxTiles = 16384;
+constexpr int64_t kNoAllocCoordBytes = ((kNoAllocMaxTiles + 1) * 2 * 8 + 255) / 256 * 256;
+constexpr int64_t kNoAllocBytes = kNoAllocCoordBytes + (kNoAllocMaxTiles * 8 + 255) / 256 * 256 +
+                                  2 * ((kNoAllocMaxTiles * 16 + 255) / 256 * 256);
+static __device__ __align__(256) unsigned char g_spmv_noalloc_scratch[kNoAllocBytes];
+
+namespace {
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mutex;
+void* g_noalloc_ptr[kMaxDevices] = {};
+
+// Device address of the scratch array for the current device (set up once).
+int noalloc_scratch(void** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+        fsb_host::set_error("fsb_spmv_csr_noalloc: no usable current device (%s)", cudaGetErrorString(e));
+        return FSB_ERR_LAUNCH;
+    }
+    std::lock_guard<std::mutex> lock(g_noalloc_mutex);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_spmv_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            fsb_host::set_error("fsb_spmv_csr_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return FSB_ERR_LAUNCH;
+        }
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return FSB_OK;
+}
+}  // namespace
+
+extern "C" int fsb_spmv_csr_noalloc(const fsb_csr* A, const void* x, void* y, int out_dtype, int acc_mode,
+                                    int32_t items_per_unit, void* stream) {
+    if (!A) {
+        fsb_host::set_error("fsb_spmv_csr_noalloc: null matrix");
+        return FSB_ERR_INVALID;
+    }
+    if (A->n_rows < 0 || A->nnz < 0) {
+        fsb_host::set_error("fsb_spmv_csr_noalloc: negative size");
+        return FSB_ERR_INVALID;
+    }
+    if (items_per_unit % kMergeThreads || items_per_unit < kMergeThreads || items_per_unit > kMergeMaxTile) {
+        fsb_host::set_error("fsb_spmv_csr_noalloc: items_per_unit=%d must be %d x [1, %d]", items_per_unit,
+                            kMergeThreads, kMergeMaxItemsPerThread);
+        return FSB_ERR_INVALID;
+    }
+    if (A->n_rows == 0) return FSB_OK;
+    const int64_t n_tiles = ceil_div(A->n_rows + A->nnz, items_per_unit);
+    if (n_tiles > kNoAllocMaxTiles) {
+        fsb_host::set_error("fsb_spmv_csr_noalloc: %lld tiles exceed the fixed scratch of %lld tiles "
+                            "(n_rows + nnz must be <= %lld at items_per_unit=%d)",
+                            (long long)n_tiles, (long long)kNoAllocMaxTiles,
+                            (long long)(kNoAllocMaxTiles * items_per_unit), items_per_unit);
+        return FSB_ERR_LIMIT;
+    }
+    if (!A->row_ptr || !y || (A->nnz > 0 && (!A->values || !A->col_idx || !x))) {
+        fsb_host::set_error("fsb_spmv_csr_noalloc: null data pointer");
+        return FSB_ERR_INVALID;
+    }
+    if (A->row_map && A->row_map_dtype != A->index_dtype) {
+        fsb_host::set_error("fsb_spmv_csr_noalloc: row_map dtype must equal index dtype");
+        return FSB_ERR_INVALID;
+    }
+    void* scratch = nullptr;
+    int rc = noalloc_scratch(&scratch);
+    if (rc) return rc;
+    int64_t* coords = static_cast<int64_t*>(scratch);
+    void* carries = static_cast<unsigned char*>(scratch) + kNoAllocCoordBytes;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return dispatch_vao(A->value_dtype, acc_mode, out_dtype, [&](auto tv, auto ta, auto to) -> int {
+        using V = typename decltype(tv)::type;
+        using Ac = typename decltype(ta)::type;
+        using O = typename decltype(to)::type;
+        return dispatch_idx(A->index_dtype, [&](auto ti) -> int {
+            using I = typename decltype(ti)::type;
+            return dispatch_idx(A->ptr_dtype, [&](auto tp) -> int {
+                using P = typename decltype(tp)::type;
+                const P* ptr = static_cast<const P*>(A->row_ptr);
+                k_merge_partition<P><<<(unsigned)ceil_div(n_tiles + 1, 256), 256, 0, st>>>(
+                    ptr, A->n_rows, A->nnz, items_per_unit, 0, coords, n_tiles);
+                int rc2 = fsb_host::check_launch("k_merge_partition (noalloc)");
+                if (rc2) return rc2;
+                MergeScratch ms = merge_scratch_carve(carries, n_tiles, 1, (int)sizeof(Ac));
+                O* yv = static_cast<O*>(y);
+                const I* rmap = static_cast<const I*>(A->row_map);
+                k_spmv_merge<V, Ac, O, I, P><<<(unsigned)n_tiles, kMergeThreads, 0, st>>>(
+                    static_cast<const V*>(A->values), static_cast<const I*>(A->col_idx), ptr, rmap,
+                    static_cast<const V*>(x), yv, A->n_rows, coords, items_per_unit / kMergeThreads, ms.carry_row,
+                    static_cast<Ac*>(ms.carry_val), static_cast<Ac*>(ms.head_val));
+                rc2 = fsb_host::check_launch("k_spmv_merge (noalloc)");
+                if (rc2) return rc2;
+                k_spmv_merge_fixup<Ac, O, I, P><<<(unsigned)ceil_div(n_tiles, 256), 256, 0, st>>>(
+                    ms.carry_row, static_cast<const Ac*>(ms.carry_val), static_cast<const Ac*>(ms.head_val),
+                    n_tiles, ptr, rmap, yv);
+                return fsb_host::check_launch("k_spmv_merge_fixup (noalloc)");
             });
         });
     });

@@ -133,6 +133,21 @@ int fsb_merge_partition(const void* row_ptr, int ptr_dtype, int64_t n_rows,
                         int64_t snap_threshold, int64_t* unit_coords,
                         int64_t n_units, void* stream);
 
+/* Allocation-free merge-path SpMV, y = A x, for callers that cannot allocate
+ * device memory (a C program or plug-in handed device pointers by a host
+ * framework that owns all device memory, or a latency-critical loop that
+ * cannot afford cudaMalloc's implicit synchronisation).  No counterpart in
+ * FlagSparse.  Same arguments and results as fsb_spmv_csr with a merge-path
+ * plan of items_per_unit items per tile (128 x [1, 8], unsnapped), but the
+ * tile coordinates and carries live in a fixed device array inside the
+ * library (about 0.9 MB, held by every GPU that loads the library until
+ * exit): at most 16384 tiles, i.e. n_rows + nnz <= 16384 * items_per_unit,
+ * else FSB_ERR_LIMIT.  Calls whose kernels overlap on the GPU race on the
+ * shared array.  The first call on a device resolves the array's address
+ * with that device current and should come before any stream capture.     */
+int fsb_spmv_csr_noalloc(const fsb_csr* A, const void* x, void* y, int out_dtype,
+                         int acc_mode, int32_t items_per_unit, void* stream);
+
 /* y = A x.  out_dtype is value_dtype, or FSB_F32 for f16/bf16 values (the
  * precision form).  y must be zero-filled by the caller when row_map is set
  * (rows without a run are not written).
