@@ -55,7 +55,7 @@ def parse_args(argv=None):
                     help="only warm-up + timed device steps (for a profiler launch list)")
     ap.add_argument("--plan", default=None,
                     help="force the chosen-form plan: rows:<lanes>[:<n_tile>] | merge:<items>:<snap> | "
-                         "flat|gather:<items>:<snap>[:<n_tile>]")
+                         "flat|gather|seq:<items>:<snap>[:<n_tile>]")
     return ap.parse_args(argv)
 
 
@@ -339,6 +339,8 @@ class SpmvPoisson:
                 fs.flagsparse_spmv_csr(x=self.x, prepared=self.prepared, out=self.y, use_opt=use_opt)
         return g
 
+    plain_desc = "float64 accumulation (FlagSparse plain), graph of 1000"
+
     def config(self):
         return {"workload": "csr_spmv_poisson16_16384x16384_f32_i32_graph1000", "n_rows": self.shape[0],
                 "nnz": self.nnz, "global_batch": self.graph_iters,
@@ -399,7 +401,167 @@ class SpmvPoisson:
         return run, per_call * 100, "100 calls of the full SpMV"
 
 
-WORKLOADS = {"spmm_powerlaw": SpmmPowerlaw, "spmv_poisson": SpmvPoisson}
+class PrecisionBanded:
+    """Precision form vs plain: 1,048,576-row banded-plus-random CSR (band 64
+    + 4 uniform off-band columns, 1 % of rows with 8192 nonzeros).  Headline:
+    bfloat16 SpMM (N = 32, float32 accumulation and output, compensated rows
+    > 4096 nonzeros); beside it bfloat16 SpMV, the float16 runs and the
+    float32 forms, each with its error against FP64 of the float32 data."""
+
+    metric = "bf16-value CSR SpMM useful throughput (precision form)"
+    unit = "GB/s"
+    n_dense = 32
+    plain_desc = "float32 values, float32 accumulation (same kernels)"
+
+    def __init__(self, n_rows=1048576):
+        self.n_rows = n_rows
+
+    def generate(self, device):
+        from flagsparse_public_b200 import synthetic
+
+        data, indices, indptr, shape = synthetic.banded_plus_random(self.n_rows, seed=0, dtype=torch.float32,
+                                                                   device=device)
+        self.A = (data, indices, indptr)
+        self.shape = shape
+        self.x = synthetic.dense_vector(shape[1], seed=1, device=device)
+        self.B = synthetic.dense_operand(shape[1], self.n_dense, seed=2, device=device)
+        self.nnz = data.numel()
+        n, N = shape[0], self.n_dense
+        self.bytes = {
+            "spmm_bf16": self.nnz * 6 + n * N * 2 + n * N * 4,
+            "spmm_f32": self.nnz * 8 + n * N * 4 + n * N * 4,
+            "spmv_bf16": self.nnz * 6 + n * 2 + n * 4,
+            "spmv_f32": self.nnz * 8 + n * 4 + n * 4,
+        }
+        self.useful_bytes = self.bytes["spmm_bf16"]
+        self.plain_bytes = self.bytes["spmm_f32"]
+        self.flops = 2 * self.nnz * N
+        lens = indptr[1:] - indptr[:-1]
+        self.row_stats = {"mean_row": float(lens.float().mean()), "max_row": int(lens.max()),
+                          "rows_over_4096": int((lens > 4096).sum())}
+
+    def build(self, device):
+        import flagsparse_public_b200 as fs
+
+        self.generate(device)
+        data, indices, indptr = self.A
+        self.half = {}
+        for dt in (torch.bfloat16, torch.float16):
+            p = fs.prepare_csr_mixed(data.to(dt), indices, indptr, self.shape)
+            self.half[dt] = (p, self.x.to(dt), self.B.to(dt))
+        self.p32 = fs.prepare_spmv_csr(data, indices, indptr, self.shape)
+        self.p32mm = fs.prepare_spmm_csr_opt(data, indices, indptr, self.shape)
+        self.C = torch.empty((self.shape[0], self.n_dense), device=device)
+        self.y = torch.empty(self.shape[0], device=device)
+
+    def config(self):
+        return {"workload": f"csr_banded64_plus4_long1pct8192_{self.shape[0]}_spmm_n{self.n_dense}_bf16",
+                "n_rows": self.shape[0], "nnz": self.nnz, "n_dense": self.n_dense, "global_batch": 1,
+                "useful_bytes_per_step": self.useful_bytes, **self.row_stats,
+                "l2": "inputs larger than L2; flushed before every timed step (256 MiB write)",
+                "parallelism": "replicas"}
+
+    def _spmm_half(self, dt):
+        import flagsparse_public_b200 as fs
+
+        p, _x, Bh = self.half[dt]
+        fs.flagsparse_spmm_csr_mixed(B=Bh, prepared=p, out=self.C)
+
+    def _spmv_half(self, dt):
+        import flagsparse_public_b200 as fs
+
+        p, xh, _B = self.half[dt]
+        fs.flagsparse_spmv_csr_mixed(x=xh, prepared=p, out=self.y)
+
+    def step(self):
+        self._spmm_half(torch.bfloat16)
+
+    def plain_step(self):
+        import flagsparse_public_b200 as fs
+
+        fs.flagsparse_spmm_csr_opt(B=self.B, prepared=self.p32mm, out=self.C)
+
+    def extra_forms(self):
+        import flagsparse_public_b200 as fs
+
+        return {
+            "spmv_bf16": (lambda: self._spmv_half(torch.bfloat16), self.bytes["spmv_bf16"]),
+            "spmv_f16": (lambda: self._spmv_half(torch.float16), self.bytes["spmv_bf16"]),
+            "spmv_f32_fp32acc": (lambda: fs.flagsparse_spmv_csr(x=self.x, prepared=self.p32, out=self.y,
+                                                                use_opt=True), self.bytes["spmv_f32"]),
+            "spmv_f32_plain": (lambda: fs.flagsparse_spmv_csr(x=self.x, prepared=self.p32, out=self.y),
+                               self.bytes["spmv_f32"]),
+            "spmm_f16": (lambda: self._spmm_half(torch.float16), self.bytes["spmm_bf16"]),
+            "spmm_f32_fp32acc": (self.plain_step, self.bytes["spmm_f32"]),
+        }
+
+    def plan_desc(self):
+        from flagsparse_public_b200.sparse_operations.precision import _mixed_plan
+
+        return _mixed_plan(self.half[torch.bfloat16][0], "spmm", self.n_dense).describe()
+
+    def force_plan(self, plan):
+        self.half[torch.bfloat16][0]._plans[("spmm", self.n_dense)] = plan
+
+    def host_inputs(self):
+        data, indices, indptr = self.A
+        self.h = [data.to(torch.bfloat16).cpu().pin_memory(), indices.cpu().pin_memory(), indptr.cpu().pin_memory(),
+                  self.B.to(torch.bfloat16).cpu().pin_memory()]
+        self.h_out = torch.empty(self.C.shape, dtype=torch.float32).pin_memory()
+        self.h2d_bytes = sum(t.numel() * t.element_size() for t in self.h)
+        self.d2h_bytes = self.h_out.numel() * self.h_out.element_size()
+
+    def e2e_step(self, device):
+        import flagsparse_public_b200 as fs
+
+        d = [t.to(device, non_blocking=True) for t in self.h]
+        C = fs.flagsparse_spmm_csr_mixed(d[0], d[1], d[2], d[3], self.shape)
+        self.h_out.copy_(C, non_blocking=True)
+
+    def fp64_error(self):
+        """Errors vs FP64 of the float32 data (storage rounding + arithmetic),
+        and of the same half inputs (arithmetic only), on a row sample."""
+        from oracle import oracle as orc
+        from tests.numerics import scaled_error
+
+        data, indices, indptr = self.A
+        rows = torch.arange(0, self.shape[0], 97, device=data.device)  # ~10.8 K rows incl. long ones
+        lens = indptr[rows + 1] - indptr[rows]
+        sub_ptr = torch.zeros(rows.numel() + 1, dtype=torch.int64, device=data.device)
+        sub_ptr[1:] = torch.cumsum(lens, 0)
+        gather = torch.repeat_interleave(indptr[rows] - sub_ptr[:-1], lens) + torch.arange(int(sub_ptr[-1]),
+                                                                                             device=data.device)
+        sub = (data[gather].cpu(), indices[gather].cpu(), sub_ptr.cpu())
+        out = {}
+        exact, mag = orc.spmm_csr_exact(*sub, self.B.cpu())
+        for dt, name in ((torch.bfloat16, "bf16"), (torch.float16, "f16")):
+            self._spmm_half(dt)
+            got = self.C[rows].cpu()
+            ex_h, mag_h = orc.spmm_csr_exact(sub[0].to(dt), sub[1], sub[2], self.B.cpu().to(dt))
+            out[f"spmm_{name}_vs_fp64_of_f32_data"] = scaled_error(got, exact, mag)
+            out[f"spmm_{name}_vs_fp64_same_inputs"] = scaled_error(got, ex_h, mag_h)
+        self.plain_step()
+        out["spmm_f32_fp32acc"] = scaled_error(self.C[rows].cpu(), exact, mag)
+        out["definition"] = "max |c - c64| / sum_k |a_k b_k| over every 97th row"
+        return out
+
+    def cpu_step_factory(self, threads, sample_rows=None):
+        from oracle import oracle as orc
+
+        data, indices, indptr = self.A
+        rows = min(self.shape[0], 65536 if sample_rows is None else sample_rows)
+        k = int(indptr[rows])
+        sub = (data[:k].to(torch.bfloat16).cpu(), indices[:k].cpu(), indptr[: rows + 1].cpu())
+        B = self.B.to(torch.bfloat16).cpu()
+        nbytes = k * 6 + self.shape[1] * self.n_dense * 2 + rows * self.n_dense * 4
+
+        def run():
+            orc.spmm_csr(*sub, B, acc_mode=orc.ACC_NATIVE, out_dtype=torch.float32, threads=threads)
+
+        return run, nbytes, f"rows [0, {rows}) ({k} nonzeros), bf16 inputs, f32 accumulation, N = {self.n_dense}"
+
+
+WORKLOADS = {"spmm_powerlaw": SpmmPowerlaw, "spmv_poisson": SpmvPoisson, "precision_banded": PrecisionBanded}
 
 
 # ------------------------------------------------------------------ timing --
@@ -474,7 +636,7 @@ def parse_plan(text):
     kind, nums = parts[0], [int(v) for v in parts[1:]]
     if kind == "rows":
         return _plan.KernelPlan(nat.ALGO_ROWS, lanes=nums[0], n_tile=nums[1] if len(nums) > 1 else 0)
-    algo = {"merge": nat.ALGO_MERGE, "flat": nat.ALGO_FLAT, "gather": nat.ALGO_GATHER}[kind]
+    algo = {"merge": nat.ALGO_MERGE, "flat": nat.ALGO_FLAT, "gather": nat.ALGO_GATHER, "seq": nat.ALGO_SEQ}[kind]
     return _plan.KernelPlan(algo, items_per_unit=nums[0], snap=nums[1] if len(nums) > 1 else 0,
                             n_tile=nums[2] if len(nums) > 2 else 0)
 
@@ -519,7 +681,19 @@ def run_ours(args):
     torch.cuda.synchronize()
     plain_times = time_device_steps(wl.plain_step, args.steps, flush)
     plain_ms = max_over_ranks(sum(plain_times), world) / args.steps
-    plain_value = wl.useful_bytes * world / (plain_ms * 1e-3) / 1e9
+    plain_value = getattr(wl, "plain_bytes", wl.useful_bytes) * world / (plain_ms * 1e-3) / 1e9
+
+    extra = {}
+    if hasattr(wl, "extra_forms"):
+        for name, (fn, nbytes) in wl.extra_forms().items():
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            ms_x = max_over_ranks(sum(time_device_steps(fn, args.steps, flush)), world) / args.steps
+            extra[name] = {"ms_per_step": ms_x, "value": nbytes * world / (ms_x * 1e-3) / 1e9, "unit": wl.unit}
+        extra["speedup_spmm_bf16_vs_f32"] = plain_ms / ms_step
+        if "spmv_bf16" in extra:
+            extra["speedup_spmv_bf16_vs_f32"] = extra["spmv_f32_fp32acc"]["ms_per_step"] / extra["spmv_bf16"]["ms_per_step"]
 
     e2e = None
     if not args.no_e2e:
@@ -566,7 +740,9 @@ def run_ours(args):
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                          "what": "useful bytes / mean CUDA-event duration of one product call"},
             "plain": {"value": plain_value, "unit": wl.unit, "ms_per_step": plain_ms,
-                      "frac": plain_value / world / peak, "accumulation": "float64 (FlagSparse plain)"},
+                      "frac": plain_value / world / peak, "form": getattr(wl, "plain_desc",
+                                                                          "float64 accumulation (FlagSparse plain)")},
+            "forms": extra or None,
             "error_vs_fp64": errors,
             "e2e": e2e,
             "cpu_baseline": cpu,

@@ -32,6 +32,10 @@ _EXPORTS = {
     "flagsparse_spmm_csr_opt": "spmm_csr",
     "flagsparse_spmm_csr_opt_alg2": "spmm_csr_opt_alg2",
     "flagsparse_spmm_coo": "spmm_coo",
+    "PreparedCsrMixed": "precision",
+    "prepare_csr_mixed": "precision",
+    "flagsparse_spmv_csr_mixed": "precision",
+    "flagsparse_spmm_csr_mixed": "precision",
 }
 
 __all__ = sorted(_EXPORTS)

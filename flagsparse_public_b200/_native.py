@@ -13,7 +13,8 @@ import threading
 import torch
 
 PKG_DIR = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG_DIR, "libflagsparse_b200.so")
+# FSB_LIB_PATH selects another build of the same library (same ABI).
+LIB_PATH = os.environ.get("FSB_LIB_PATH") or os.path.join(PKG_DIR, "libflagsparse_b200.so")
 
 FSB_OK = 0
 FSB_ERR_INVALID = -1
@@ -25,7 +26,7 @@ FSB_ERR_LIMIT = -6
 
 FSB_F16, FSB_BF16, FSB_F32, FSB_F64, FSB_C64, FSB_C128, FSB_I32, FSB_I64 = range(8)
 ACC_NATIVE, ACC_WIDE, ACC_COMP = 0, 1, 2
-ALGO_ROWS, ALGO_MERGE, ALGO_FLAT, ALGO_GATHER = 0, 1, 2, 3
+ALGO_ROWS, ALGO_MERGE, ALGO_FLAT, ALGO_GATHER, ALGO_SEQ = 0, 1, 2, 3, 4
 
 _DTYPE_CODES = {
     torch.float16: FSB_F16,
@@ -195,7 +196,7 @@ def make_csr(values, col_idx, row_ptr, n_rows, n_cols, row_map=None):
 
 
 def make_plan(algo, lanes=32, items_per_unit=0, n_tile=0, coords=None, n_units=0, row_cap=0, comp_threshold=0,
-              grid_blocks=0):
+              grid_blocks=0, flags=0):
     p = FsbPlan()
     p.algo = int(algo)
     p.lanes = int(lanes)
@@ -206,5 +207,5 @@ def make_plan(algo, lanes=32, items_per_unit=0, n_tile=0, coords=None, n_units=0
     p.row_cap = int(row_cap)
     p.comp_threshold = int(comp_threshold)
     p.grid_blocks = int(grid_blocks)
-    p.flags = 0
+    p.flags = int(flags)
     return p

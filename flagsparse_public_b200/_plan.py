@@ -93,7 +93,7 @@ class KernelPlan:
             kind = "warp_rows" if self.lanes == 32 else "vector_rows"
             return {"kind": kind, "lanes": self.lanes, "n_tile": self.n_tile}
         kind = {nat.ALGO_MERGE: "merge_path", nat.ALGO_FLAT: "merge_path_flat",
-                nat.ALGO_GATHER: "merge_path_tma_gather"}[self.algo]
+                nat.ALGO_GATHER: "merge_path_tma_gather", nat.ALGO_SEQ: "merge_path_seq"}[self.algo]
         return {"kind": kind, "items_per_unit": self.items_per_unit, "n_tile": self.n_tile,
                 "snap": self.snap, "n_units": self.n_units}
 
@@ -147,25 +147,24 @@ def default_spmv_plan(stats, dtype, row_cap=0):
     return KernelPlan(nat.ALGO_ROWS, lanes=lanes)
 
 
+SM_COUNT = 148  # B200
+SEQ_WARPS_PER_SM = 32
+
+
+def seq_items_per_unit(stats):
+    """Merge-path unit size for the batched SpMM kernel: (rows + nonzeros)
+    spread over about two waves of resident warps, between 128 and 1024."""
+    items = stats.n_rows + stats.nnz
+    return _pow2_clamp(items / (SM_COUNT * SEQ_WARPS_PER_SM * 2), 128, 1024)
+
+
 def default_spmm_plan(stats, n_dense, dtype, row_cap=0):
-    """Heuristic SpMM plan: merge path (row-aligned units, long rows split) for
-    skewed rows; warp per row for medium rows; vector per row for short rows."""
+    """Heuristic SpMM plan: the batched merge-path kernel (nonzero-balanced
+    units, rows split across units where long); row groups when a per-row
+    segment cap is requested."""
     if row_cap > 0 or stats.n_rows == 0:
         return KernelPlan(nat.ALGO_ROWS, lanes=32, row_cap=row_cap)
-    elem = torch.empty((), dtype=dtype).element_size()
-    vw = max(1, 16 // max(elem, 4 if dtype in (torch.float16, torch.bfloat16) else elem))
-    if n_dense >= 8 * vw and (n_dense * elem) % 16 == 0:
-        # TMA bulk gathers of B rows (falls back to the register-staged flat
-        # kernel at run time when B / C rows are not 16-byte aligned)
-        return KernelPlan(nat.ALGO_GATHER, items_per_unit=256, fallback_ok=True)
-    if n_dense >= 8:
-        return KernelPlan(nat.ALGO_FLAT, items_per_unit=256)
-    skewed = stats.max_row > 8 * max(stats.mean_row, 1.0) + 64
-    if skewed:
-        return KernelPlan(nat.ALGO_MERGE, items_per_unit=128, snap=64)
-    if stats.mean_row < 6:
-        return KernelPlan(nat.ALGO_ROWS, lanes=1)  # widened to one column tile's lanes
-    return KernelPlan(nat.ALGO_ROWS, lanes=32)
+    return KernelPlan(nat.ALGO_SEQ, items_per_unit=seq_items_per_unit(stats))
 
 
 def _workspace(is_spmm, cm, n_dense, acc_mode, out_code, cp, device):

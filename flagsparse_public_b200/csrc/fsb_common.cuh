@@ -49,6 +49,40 @@ __device__ __forceinline__ vec_t<T, N> ld_ro(const T* p) {
     memcpy(&out, &r, sizeof(R));
     return out;
 }
+// L2 policy that keeps lines resident (dense operands gathered many times
+// while the sparse stream passes through once).
+__device__ __forceinline__ uint64_t policy_evict_last() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_last.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+// Read-only load with an L2 cache policy (2, 4, 8 or 16 bytes).
+template <class T, int N>
+__device__ __forceinline__ vec_t<T, N> ld_keep(const T* p, uint64_t pol) {
+    constexpr int BY = (int)sizeof(T) * N;
+    vec_t<T, N> out;
+    if constexpr (BY == 2) {
+        unsigned short r;
+        asm("ld.global.nc.L2::cache_hint.u16 %0, [%1], %2;" : "=h"(r) : "l"(p), "l"(pol));
+        memcpy(&out, &r, 2);
+    } else if constexpr (BY == 4) {
+        unsigned int r;
+        asm("ld.global.nc.L2::cache_hint.u32 %0, [%1], %2;" : "=r"(r) : "l"(p), "l"(pol));
+        memcpy(&out, &r, 4);
+    } else if constexpr (BY == 8) {
+        uint2 r;
+        asm("ld.global.nc.L2::cache_hint.v2.u32 {%0, %1}, [%2], %3;" : "=r"(r.x), "=r"(r.y) : "l"(p), "l"(pol));
+        memcpy(&out, &r, 8);
+    } else {
+        static_assert(BY == 16, "ld_keep: 2, 4, 8 or 16 bytes");
+        uint4 r;
+        asm("ld.global.nc.L2::cache_hint.v4.u32 {%0, %1, %2, %3}, [%4], %5;"
+            : "=r"(r.x), "=r"(r.y), "=r"(r.z), "=r"(r.w)
+            : "l"(p), "l"(pol));
+        memcpy(&out, &r, 16);
+    }
+    return out;
+}
 template <class T>
 __device__ __forceinline__ T ld_stream1(const T* p) { return ld_stream<T, 1>(p).v[0]; }
 template <class T>

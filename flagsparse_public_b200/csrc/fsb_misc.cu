@@ -77,7 +77,9 @@ extern "C" int64_t fsb_workspace_bytes(int is_spmm, const fsb_csr* A, int64_t n_
                                        const fsb_plan* plan) {
     (void)out_dtype;
     if (!A || !plan) return 0;
-    if (plan->algo != FSB_ALGO_MERGE && plan->algo != FSB_ALGO_FLAT && plan->algo != FSB_ALGO_GATHER) return 0;
+    if (plan->algo != FSB_ALGO_MERGE && plan->algo != FSB_ALGO_FLAT && plan->algo != FSB_ALGO_GATHER &&
+        plan->algo != FSB_ALGO_SEQ)
+        return 0;
     const int ab = acc_size(A->value_dtype, acc_mode);
     if (ab == 0) return 0;
     return merge_scratch_bytes(plan->n_units, is_spmm ? n_dense : 1, ab);

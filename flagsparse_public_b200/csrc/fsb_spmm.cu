@@ -21,6 +21,7 @@
 // kernels (:778-919), the alg2 kernels (spmm_csr_opt_alg2.py:338-629) and the
 // COO row-run kernels (spmm_coo.py:135-241).
 #include "fsb_spmm_common.cuh"
+#include "fsb_spmm_seq.cuh"
 
 namespace fsb {
 
@@ -72,8 +73,6 @@ __device__ __forceinline__ void row_segment(const V* __restrict__ val, const I* 
     }
 }
 
-template <class A> struct is_comp_acc { static constexpr bool value = false; };
-template <> struct is_comp_acc<comp_t> { static constexpr bool value = true; };
 
 template <class V, class A, class I, int VW>
 __device__ __forceinline__ void row_accumulate(const V* __restrict__ val, const I* __restrict__ col,
@@ -506,6 +505,19 @@ extern "C" int fsb_spmm_csr(const fsb_csr* A, const void* B, int64_t ldb, int64_
     if (plan->algo == FSB_ALGO_GATHER)
         return spmm_gather_dispatch(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes,
                                     st);
+    if (plan->algo == FSB_ALGO_SEQ) {
+        switch (A->value_dtype) {
+        case FSB_F16: return seq_dispatch_f16(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
+        case FSB_BF16: return seq_dispatch_bf16(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
+        case FSB_F32: return seq_dispatch_f32(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
+        case FSB_F64: return seq_dispatch_f64(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
+        case FSB_C64: return seq_dispatch_c64(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
+        case FSB_C128: return seq_dispatch_c128(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
+        default:
+            fsb_host::set_error("fsb_spmm_csr: value dtype code %d", A->value_dtype);
+            return FSB_ERR_UNSUPPORTED;
+        }
+    }
     return dispatch_vao(A->value_dtype, acc_mode, out_dtype, [&](auto tv, auto ta, auto to) -> int {
         using V = typename decltype(tv)::type;
         using Ac = typename decltype(ta)::type;

@@ -21,6 +21,9 @@ __device__ __forceinline__ void store_row(O* __restrict__ C, int64_t ldc, int64_
     }
 }
 
+template <class A> struct is_comp_acc { static constexpr bool value = false; };
+template <> struct is_comp_acc<comp_t> { static constexpr bool value = true; };
+
 template <class A, int VW>
 __device__ __forceinline__ void zero_acc(A (&acc)[VW]) {
 #pragma unroll

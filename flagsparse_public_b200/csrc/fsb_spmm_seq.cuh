@@ -1,0 +1,339 @@
+// fsb_spmm_seq.cuh -- the batched merge-path SpMM kernel template and its
+// launcher (FSB_ALGO_SEQ; instantiated per value type in fsb_spmm_seq_*.cu).
+//
+// One warp per (merge-path unit, column tile).  The warp walks the unit's
+// nonzeros in order, NPAR = 32 / LPN of them per step: sub-group s (LPN lanes)
+// takes nonzero k + s and covers the column tile with VW elements per lane
+// (16-byte lane vectors where B and C allow), so a step costs each lane one
+// vector load of a B-row slice and VW fused multiply-adds.
+//
+// Batches of U steps (UN = U * NPAR nonzeros, UN divides 32) issue their U
+// B loads back to back -- independent, so all are in flight together --
+// before the accumulation uses them.  A batch lying inside one row takes the
+// unpredicated path; a batch holding row ends is consumed in segments, one
+// row each: the sub-groups add their nonzeros of the segment, the row's sum is
+// reduced across sub-groups (log2 NPAR xor-shuffles per element) and stored.
+// The row flush exists once, outside the unrolled bodies, which keeps the
+// kernel small.  B loads carry an L2 evict-last policy: B rows are gathered
+// many times while the values and column indices stream through once.
+//
+// Split rows finish through the carries shared with the other merge-path SpMM
+// kernels (k_spmm_merge_fixup).
+#pragma once
+#include <type_traits>
+
+#include "fsb_spmm_common.cuh"
+
+namespace fsb {
+
+// steps per batch: 16 B-element registers per lane, at most 32 nonzeros
+template <int VW, int NPAR> struct SeqBatch {
+    static constexpr int by_regs = 16 / VW < 1 ? 1 : 16 / VW;
+    static constexpr int value = by_regs * NPAR > 32 ? 32 / NPAR : by_regs;
+};
+
+template <class V, class A, class O, class I, class P, int VW, int LPN_LOG2, bool ADDR32>
+__global__ void __launch_bounds__(kSpmmThreads, 8)
+k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __restrict__ ptr,
+           const I* __restrict__ row_map, const V* __restrict__ B, int64_t ldb, O* __restrict__ C, int64_t ldc,
+           int64_t n_rows, int64_t n_dense, const int64_t* __restrict__ coords, int64_t n_units,
+           int64_t comp_threshold, int64_t* __restrict__ carry_row, A* __restrict__ carry_val,
+           A* __restrict__ head_val) {
+    constexpr int kNoEnd = 0x7fffffff;
+    constexpr int LPN = 1 << LPN_LOG2;
+    constexpr int NPAR = 32 >> LPN_LOG2;
+    constexpr int U = SeqBatch<VW, NPAR>::value;
+    constexpr int UN = U * NPAR;  // nonzeros per batch (divides 32)
+    const int lane = threadIdx.x & 31;
+    const int64_t unit = (int64_t)blockIdx.x * (kSpmmThreads / 32) + (threadIdx.x >> 5);
+    if (unit >= n_units) return;  // whole warp
+    const unsigned full = 0xffffffffu;
+    const int sub = lane >> LPN_LOG2;
+    const int64_t c0 = (int64_t)blockIdx.y * (LPN * VW) + (int64_t)(lane & (LPN - 1)) * VW;
+    const bool col_ok = c0 < n_dense;
+    // lanes past the last column read column 0 (a valid address) and store nothing
+    const V* Bl = B + (col_ok ? c0 : 0);
+    const uint64_t keep_b = policy_evict_last();
+
+    const int64_t r0 = coords[2 * unit], k0 = coords[2 * unit + 1];
+    const int64_t r1 = coords[2 * unit + 2], k1 = coords[2 * unit + 3];
+    const int64_t last_row = r1 < n_rows ? r1 : r1 - 1;
+    const int nk = (int)(k1 - k0);  // unit nonzeros (the host keeps units far below 2^31)
+
+    // Row ends relative to k0; a row ending past the unit reads as kNoEnd.
+    auto load_ends = [&](int64_t rbase) -> int {
+        const int64_t r = rbase + lane;
+        if (r > last_row) return kNoEnd;
+        const int64_t e = idx(ptr[r + 1]) - k0;
+        return e > (int64_t)kNoEnd ? kNoEnd : (int)e;
+    };
+    // rows rb .. rb + 31 in e_win, the next 32 prefetched in e_nxt
+    int64_t rb = r0;
+    int e_win = load_ends(rb);
+    int e_nxt = load_ends(rb + 32);
+    int64_t row = r0;
+    int64_t row_start = (r0 < n_rows) ? idx(ptr[r0]) : k0;  // global start of the current row
+    const bool continued = (r0 < n_rows) && (k0 > row_start);
+    int row_end = __shfl_sync(full, e_win, 0);
+    // FSB_ACC_COMP: compensated accumulation only on rows longer than
+    // comp_threshold nonzeros; shorter rows add plainly into the f32 part.
+    auto row_is_long = [&]() -> bool {
+        if constexpr (!is_comp_acc<A>::value) return false;
+        if (row > last_row) return false;
+        const int64_t len = (row_end == kNoEnd ? idx(ptr[row + 1]) : k0 + row_end) - row_start;
+        return len > comp_threshold;
+    };
+    bool long_row = row_is_long();
+
+    A acc[VW];
+    zero_acc<A, VW>(acc);
+    auto fma_vec = [&](V a, const vec_t<V, VW>& b) {
+        if constexpr (is_comp_acc<A>::value) {
+            if (!long_row) {
+#pragma unroll
+                for (int w = 0; w < VW; ++w) acc[w].s = fmaf(to_f32(a), to_f32(b.v[w]), acc[w].s);
+                return;
+            }
+        }
+#pragma unroll
+        for (int w = 0; w < VW; ++w) acc[w] = Acc<V, A>::fma(a, b.v[w], acc[w]);
+    };
+    auto reduce = [&]() {
+        if constexpr (NPAR > 1) {
+#pragma unroll
+            for (int w = 0; w < VW; ++w) acc[w] = segment_reduce(full, acc[w], LPN, 32);
+        }
+    };
+    // Store the finished current row and move to the next one.
+    auto flush = [&]() {
+        reduce();
+        if (sub == 0 && col_ok) {
+            if (row == r0 && continued) {
+                A* dst = head_val + unit * n_dense + c0;
+#pragma unroll
+                for (int w = 0; w < VW; ++w) dst[w] = acc[w];
+            } else {
+                const int64_t out_row = row_map ? idx(row_map[row_start]) : row;
+                store_row<O, A, VW>(C, ldc, out_row, c0, acc);
+            }
+        }
+        zero_acc<A, VW>(acc);
+        ++row;
+        row_start = k0 + row_end;
+        if (row <= last_row && row - rb >= 32) {
+            rb += 32;
+            e_win = e_nxt;
+            e_nxt = load_ends(rb + 32);
+        }
+        row_end = row <= last_row ? __shfl_sync(full, e_win, (int)(row - rb)) : kNoEnd;
+        long_row = row_is_long();
+    };
+    auto b_row = [&](I c) -> const V* {
+        if constexpr (ADDR32) return Bl + (uint32_t)((uint32_t)c * (uint32_t)ldb);
+        else return Bl + idx(c) * ldb;
+    };
+
+    // Value / column windows: lane l holds entry kb + l (current) and
+    // kb + 32 + l (next), relative to k0.
+    int kb = 0;
+    V v_cur = vzero<V>(), v_nxt = vzero<V>();
+    I c_cur = 0, c_nxt = 0;
+    if (lane < nk) { v_cur = ld_stream1(val + k0 + lane); c_cur = ld_stream1(col + k0 + lane); }
+    if (32 + lane < nk) { v_nxt = ld_stream1(val + k0 + 32 + lane); c_nxt = ld_stream1(col + k0 + 32 + lane); }
+
+    for (int k = 0; k < nk;) {
+        // UN divides 32 and k advances by UN except at the unit end, so a batch
+        // never crosses the window: bs + u * NPAR stays below 32
+        const int n_here = nk - k < UN ? nk - k : UN;
+        const int bs = (k - kb) + sub;
+        vec_t<V, VW> bv[U];
+        if (n_here == UN) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) bv[u] = ld_keep<V, VW>(b_row(shfl_idx(full, c_cur, bs + u * NPAR, 32)), keep_b);
+        } else {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const I c = shfl_idx(full, c_cur, (bs + u * NPAR) & 31, 32);
+                if (u * NPAR + sub < n_here) {
+                    bv[u] = ld_keep<V, VW>(b_row(c), keep_b);
+                } else {
+#pragma unroll
+                    for (int w = 0; w < VW; ++w) bv[u].v[w] = vzero<V>();
+                }
+            }
+        }
+        if (n_here == UN && row_end - k >= UN) {
+            // common case: the batch lies inside the current row
+#pragma unroll
+            for (int u = 0; u < U; ++u) fma_vec(shfl_idx(full, v_cur, bs + u * NPAR, 32), bv[u]);
+        } else {
+            // segments [s, e) of the batch, one row each, flushed in between
+            int s = 0;
+            for (;;) {
+                const int e = row_end - k;
+                if (e <= s) {
+                    flush();
+                    continue;
+                }
+                const int ee = e < n_here ? e : n_here;
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const V a = shfl_idx(full, v_cur, (bs + u * NPAR) & 31, 32);
+                    const int p = u * NPAR + sub;
+                    if (p >= s && p < ee) fma_vec(a, bv[u]);
+                }
+                if (ee == n_here) break;
+                s = ee;
+            }
+        }
+        k += n_here;
+        if (k - kb == 32) {
+            kb += 32;
+            v_cur = v_nxt;
+            c_cur = c_nxt;
+            if (kb + 32 + lane < nk) {
+                v_nxt = ld_stream1(val + k0 + kb + 32 + lane);
+                c_nxt = ld_stream1(col + k0 + kb + 32 + lane);
+            }
+        }
+    }
+    while (row < r1) flush();  // rows ending at the unit end, empty rows
+    bool open = false;
+    if (r1 < n_rows) {
+        const int64_t s1 = row_start > k0 ? row_start : k0;  // row == r1 here
+        open = k1 > s1;
+        if (open) {
+            reduce();
+            if (sub == 0 && col_ok) {
+                A* dst = carry_val + unit * n_dense + c0;
+#pragma unroll
+                for (int w = 0; w < VW; ++w) dst[w] = acc[w];
+            }
+        }
+    }
+    if (blockIdx.y == 0 && lane == 0) carry_row[unit] = open ? r1 : -1;
+}
+
+// Widest lane vector: 16 bytes of B and of C.
+template <class V, class O>
+constexpr int seq_max_vw() {
+    constexpr int bv = 16 / (int)sizeof(V), bo = 16 / (int)sizeof(O);
+    return bv < bo ? bv : bo;
+}
+
+template <class V, class A, class O, class I, class P, int VW>
+void launch_seq_vw(int lpn_log2, bool addr32, dim3 g, cudaStream_t st, const V* val, const I* col, const P* ptr,
+                   const I* rmap, const V* B, int64_t ldb, O* C, int64_t ldc, int64_t n_rows, int64_t n_dense,
+                   const int64_t* coords, int64_t n_units, int64_t thr, int64_t* carry_row, A* cv, A* hv) {
+#define FSB_SEQ_LAUNCH(L)                                                                                         \
+    if (lpn_log2 == L) {                                                                                          \
+        if (addr32)                                                                                               \
+            k_spmm_seq<V, A, O, I, P, VW, L, true><<<g, kSpmmThreads, 0, st>>>(                                   \
+                val, col, ptr, rmap, B, ldb, C, ldc, n_rows, n_dense, coords, n_units, thr, carry_row, cv, hv);   \
+        else                                                                                                      \
+            k_spmm_seq<V, A, O, I, P, VW, L, false><<<g, kSpmmThreads, 0, st>>>(                                  \
+                val, col, ptr, rmap, B, ldb, C, ldc, n_rows, n_dense, coords, n_units, thr, carry_row, cv, hv);   \
+        return;                                                                                                   \
+    }
+    FSB_SEQ_LAUNCH(0)
+    FSB_SEQ_LAUNCH(1)
+    FSB_SEQ_LAUNCH(2)
+    FSB_SEQ_LAUNCH(3)
+    FSB_SEQ_LAUNCH(4)
+    FSB_SEQ_LAUNCH(5)
+#undef FSB_SEQ_LAUNCH
+}
+
+template <class V, class A, class O, class I, class P>
+int launch_seq(const fsb_csr* Am, const V* val, const I* col, const P* ptr, const I* rmap, const V* B, int64_t ldb,
+               int64_t n_dense, O* C, int64_t ldc, const fsb_plan* plan, void* workspace, int64_t workspace_bytes,
+               cudaStream_t st) {
+    const int64_t n_units = plan->n_units;
+    if (plan->items_per_unit < 1 || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
+        !plan->unit_coords || plan->row_cap > 0) {
+        fsb_host::set_error("fsb_spmm_csr: seq plan does not match the matrix");
+        return FSB_ERR_INVALID;
+    }
+    // Lane vectors of the widest aligned width (whole vectors: n_dense a
+    // multiple of the width); otherwise one element per lane.
+    constexpr int kMaxVW = seq_max_vw<V, O>();
+    const bool wide_ok = ((uintptr_t)B) % (kMaxVW * sizeof(V)) == 0 && ldb % kMaxVW == 0 &&
+                         n_dense % kMaxVW == 0 && ((uintptr_t)C) % (kMaxVW * sizeof(O)) == 0 && ldc % kMaxVW == 0;
+    const int vw = wide_ok ? kMaxVW : 1;
+    // Lanes per nonzero: the column tile (n_tile, or all of n_dense) in lane
+    // vectors, rounded up to a power of two, at most 32.
+    const int64_t target = plan->n_tile > 0 ? plan->n_tile : n_dense;
+    int lpn_log2 = 0;
+    while ((int64_t)(vw << lpn_log2) < target && lpn_log2 < 5) ++lpn_log2;
+    const int64_t need = merge_scratch_bytes(n_units, n_dense, (int)sizeof(A));
+    if (!workspace || workspace_bytes < need) {
+        fsb_host::set_error("fsb_spmm_csr: workspace %lld bytes < %lld", (long long)workspace_bytes, (long long)need);
+        return FSB_ERR_WORKSPACE;
+    }
+    const int64_t col_tiles = ceil_div(n_dense, (int64_t)(vw << lpn_log2));
+    const int64_t blocks = ceil_div(n_units, kSpmmThreads / 32);
+    if (col_tiles > 65535 || blocks > 0x7fffffffLL) {
+        fsb_host::set_error("fsb_spmm_csr: seq grid too large");
+        return FSB_ERR_LIMIT;
+    }
+    // 32-bit B offsets when every row start fits (unsigned arithmetic)
+    const bool addr32 = Am->n_cols * ldb + n_dense < 0xffffffffLL;
+    MergeScratch ms = merge_scratch_carve(workspace, n_units, n_dense, (int)sizeof(A));
+    A* cv = static_cast<A*>(ms.carry_val);
+    A* hv = static_cast<A*>(ms.head_val);
+    const int64_t thr = plan->comp_threshold > 0 ? plan->comp_threshold : 0;
+    dim3 g((unsigned)blocks, (unsigned)col_tiles);
+    if (vw == kMaxVW)
+        launch_seq_vw<V, A, O, I, P, kMaxVW>(lpn_log2, addr32, g, st, val, col, ptr, rmap, B, ldb, C, ldc, Am->n_rows,
+                                             n_dense, plan->unit_coords, n_units, thr, ms.carry_row, cv, hv);
+    if constexpr (kMaxVW > 1) {
+        if (vw == 1)
+            launch_seq_vw<V, A, O, I, P, 1>(lpn_log2, addr32, g, st, val, col, ptr, rmap, B, ldb, C, ldc, Am->n_rows,
+                                            n_dense, plan->unit_coords, n_units, thr, ms.carry_row, cv, hv);
+    }
+    int rc = fsb_host::check_launch("k_spmm_seq");
+    if (rc) return rc;
+    k_spmm_merge_fixup<A, O, I, P><<<(unsigned)blocks, kSpmmThreads, 0, st>>>(
+        ms.carry_row, static_cast<const A*>(ms.carry_val), static_cast<const A*>(ms.head_val), n_units, n_dense, ptr,
+        rmap, C, ldc);
+    return fsb_host::check_launch("k_spmm_merge_fixup");
+}
+
+// Launch for value type VSel only (each fsb_spmm_seq_*.cu instantiates one).
+template <class VSel>
+int seq_dispatch_for(const fsb_csr* A, const void* B, int64_t ldb, int64_t n_dense, void* C, int64_t ldc,
+                     int out_dtype, int acc_mode, const fsb_plan* plan, void* workspace, int64_t workspace_bytes,
+                     cudaStream_t st) {
+    return dispatch_vao(A->value_dtype, acc_mode, out_dtype, [&](auto tv, auto ta, auto to) -> int {
+        using V = typename decltype(tv)::type;
+        using Ac = typename decltype(ta)::type;
+        using O = typename decltype(to)::type;
+        if constexpr (!std::is_same<V, VSel>::value) {
+            return FSB_ERR_UNSUPPORTED;
+        } else {
+            return dispatch_idx(A->index_dtype, [&](auto ti) -> int {
+                using I = typename decltype(ti)::type;
+                return dispatch_idx(A->ptr_dtype, [&](auto tp) -> int {
+                    using P = typename decltype(tp)::type;
+                    return launch_seq<V, Ac, O, I, P>(
+                        A, static_cast<const V*>(A->values), static_cast<const I*>(A->col_idx),
+                        static_cast<const P*>(A->row_ptr), static_cast<const I*>(A->row_map),
+                        static_cast<const V*>(B), ldb, n_dense, static_cast<O*>(C), ldc, plan, workspace,
+                        workspace_bytes, st);
+                });
+            });
+        }
+    });
+}
+
+#define FSB_SEQ_DECL(NAME)                                                                                       \
+    int NAME(const fsb_csr* A, const void* B, int64_t ldb, int64_t n_dense, void* C, int64_t ldc, int out_dtype, \
+             int acc_mode, const fsb_plan* plan, void* workspace, int64_t workspace_bytes, cudaStream_t st)
+FSB_SEQ_DECL(seq_dispatch_f16);
+FSB_SEQ_DECL(seq_dispatch_bf16);
+FSB_SEQ_DECL(seq_dispatch_f32);
+FSB_SEQ_DECL(seq_dispatch_f64);
+FSB_SEQ_DECL(seq_dispatch_c64);
+FSB_SEQ_DECL(seq_dispatch_c128);
+
+}  // namespace fsb

@@ -63,6 +63,11 @@ extern "C" {
 #define FSB_ALGO_GATHER 3  /* SpMM: merge-path units, B rows gathered into a
                               shared-memory ring by TMA bulk copies
                               (cp.async.bulk + mbarrier), several stages deep */
+#define FSB_ALGO_SEQ    4  /* SpMM: merge-path units, the warp walks a unit's
+                              nonzeros in batches of up to 32 (32 / LPN per
+                              step, 16-byte lane vectors over a column tile),
+                              B rows gathered to registers, rows reduced
+                              across sub-groups only at row ends            */
 
 /* A CSR matrix (or a sorted COO matrix seen as row runs).
  * row_ptr has n_rows + 1 entries.  If row_map is non-null, row r of this

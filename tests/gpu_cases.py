@@ -65,7 +65,9 @@ def spmm_plans():
     plans += [_plan.KernelPlan(nat.ALGO_FLAT, items_per_unit=ipu, snap=snap, n_tile=nt)
               for ipu, snap, nt in ((16, 0, 0), (100, 0, 0), (256, 128, 0), (1024, 0, 0), (128, 64, 32))]
     plans += [_plan.KernelPlan(nat.ALGO_GATHER, items_per_unit=ipu, snap=snap, n_tile=nt)
-              for ipu, snap, nt in ((16, 0, 0), (100, 0, 0), (256, 128, 0), (2048, 0, 0), (128, 64, 32))]
+              for ipu, snap, nt in ((16, 0, 0), (100, 0, 0), (256, 128, 0), (2048, 0, 0), (128, 64, 32), (64, 0, 0))]
+    plans += [_plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=ipu, snap=snap, n_tile=nt)
+              for ipu, snap, nt in ((16, 0, 0), (100, 0, 0), (256, 128, 0), (2048, 0, 0), (128, 64, 32), (77, 0, 8))]
     return plans
 
 

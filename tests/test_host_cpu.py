@@ -176,8 +176,11 @@ def test_default_plans():
     skew = _plan.MatrixStats(262144, 262144, 3_100_000, 7200, 11.9, 80.0, 10)
     assert _plan.default_spmv_plan(skew, torch.float32).algo == nat.ALGO_MERGE
     mm = _plan.default_spmm_plan(skew, 64, torch.float32)
-    assert mm.algo == nat.ALGO_GATHER and mm.items_per_unit > 0 and mm.fallback_ok
-    assert mm.as_flat().algo == nat.ALGO_FLAT
-    assert _plan.default_spmm_plan(skew, 4, torch.float32).algo == nat.ALGO_MERGE
+    assert mm.algo == nat.ALGO_SEQ and mm.items_per_unit == 256
+    assert _plan.default_spmm_plan(skew, 4, torch.float32).algo == nat.ALGO_SEQ
+    banded = _plan.MatrixStats(1 << 20, 1 << 20, 156_953_476, 8192, 149.7, 780.0, 0)
+    assert _plan.default_spmm_plan(banded, 32, torch.bfloat16).items_per_unit == 1024
+    g = _plan.KernelPlan(nat.ALGO_GATHER, items_per_unit=256, fallback_ok=True)
+    assert g.as_flat().algo == nat.ALGO_FLAT
     capped = _plan.default_spmv_plan(skew, torch.float32, row_cap=32)
     assert capped.algo == nat.ALGO_ROWS and capped.row_cap == 32
