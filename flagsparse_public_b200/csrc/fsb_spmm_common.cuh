@@ -10,7 +10,18 @@ constexpr int kSpmmThreads = 128;
 template <class O, class A, int VW>
 __device__ __forceinline__ void store_row(O* __restrict__ C, int64_t ldc, int64_t out_row, int64_t c0,
                                           const A (&acc)[VW]) {
-    if constexpr (VW > 1 && (sizeof(O) * VW == 16 || sizeof(O) * VW == 8 || sizeof(O) * VW == 4)) {
+    if constexpr (VW > 1 && sizeof(O) * VW == 32) {
+        // two 16-byte halves
+        constexpr int H = VW / 2;
+        vec_t<O, H> lo, hi;
+#pragma unroll
+        for (int w = 0; w < H; ++w) {
+            lo.v[w] = Out<O, A>::cvt(acc[w]);
+            hi.v[w] = Out<O, A>::cvt(acc[H + w]);
+        }
+        st_stream<O, H>(C + out_row * ldc + c0, lo);
+        st_stream<O, H>(C + out_row * ldc + c0 + H, hi);
+    } else if constexpr (VW > 1 && (sizeof(O) * VW == 16 || sizeof(O) * VW == 8 || sizeof(O) * VW == 4)) {
         vec_t<O, VW> o;
 #pragma unroll
         for (int w = 0; w < VW; ++w) o.v[w] = Out<O, A>::cvt(acc[w]);

@@ -26,14 +26,27 @@
 
 namespace fsb {
 
-// steps per batch: 16 B-element registers per lane, at most 32 nonzeros
-template <int VW, int NPAR> struct SeqBatch {
-    static constexpr int by_regs = 16 / VW < 1 ? 1 : 16 / VW;
-    static constexpr int value = by_regs * NPAR > 32 ? 32 / NPAR : by_regs;
+// Resident CTAs per SM requested from the compiler (register cap 65536 /
+// (128 x blocks)): 8 (64 registers) while a lane's accumulators take at most
+// 16 bytes, 6 (80 registers) up to 48 bytes (block-compensated rows add a
+// 4-byte partial per element), else 4.  Gathers are latency bound, so
+// resident warps are worth more than the few bytes ptxas spills at 64.
+template <class V, class A, int VW> struct SeqMinBlocks {
+    static constexpr int acc_bytes =
+        (int)sizeof(A) * VW + ((is_comp_acc<A>::value && sizeof(V) == 2) ? 4 * VW : 0);
+    static constexpr int value = acc_bytes <= 16 ? 8 : (acc_bytes <= 48 ? 6 : 4);
+};
+
+// Steps per batch: 16 B elements per lane in flight at 8 resident CTAs, 32 at
+// fewer (fewer warps need more loads each), at most 32 nonzeros per batch.
+template <class V, class A, int VW, int NPAR> struct SeqBatch {
+    static constexpr int elems = SeqMinBlocks<V, A, VW>::value >= 8 ? 16 : 32;
+    static constexpr int by_elems = elems / VW < 1 ? 1 : elems / VW;
+    static constexpr int value = by_elems * NPAR > 32 ? 32 / NPAR : by_elems;
 };
 
 template <class V, class A, class O, class I, class P, int VW, int LPN_LOG2, bool ADDR32>
-__global__ void __launch_bounds__(kSpmmThreads, 8)
+__global__ void __launch_bounds__(kSpmmThreads, SeqMinBlocks<V, A, VW>::value)
 k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __restrict__ ptr,
            const I* __restrict__ row_map, const V* __restrict__ B, int64_t ldb, O* __restrict__ C, int64_t ldc,
            int64_t n_rows, int64_t n_dense, const int64_t* __restrict__ coords, int64_t n_units,
@@ -42,7 +55,11 @@ k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __rest
     constexpr int kNoEnd = 0x7fffffff;
     constexpr int LPN = 1 << LPN_LOG2;
     constexpr int NPAR = 32 >> LPN_LOG2;
-    constexpr int U = SeqBatch<VW, NPAR>::value;
+    constexpr int U = SeqBatch<V, A, VW, NPAR>::value;
+    // Compensated rows with 16-bit values: the products are exact in f32, so
+    // a batch's products are summed plainly (per lane, at most U of them) and
+    // the batch sum enters the (s, c) accumulator through one TwoSum.
+    constexpr bool kBlockComp = is_comp_acc<A>::value && sizeof(V) == 2;
     constexpr int UN = U * NPAR;  // nonzeros per batch (divides 32)
     const int lane = threadIdx.x & 31;
     const int64_t unit = (int64_t)blockIdx.x * (kSpmmThreads / 32) + (threadIdx.x >> 5);
@@ -97,6 +114,35 @@ k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __rest
         }
 #pragma unroll
         for (int w = 0; w < VW; ++w) acc[w] = Acc<V, A>::fma(a, b.v[w], acc[w]);
+    };
+    // Per-batch partial sums of the block-compensated rows.
+    float blk[kBlockComp ? VW : 1];
+    auto blk_zero = [&]() {
+        if constexpr (kBlockComp) {
+#pragma unroll
+            for (int w = 0; w < VW; ++w) blk[w] = 0.f;
+        }
+    };
+    // One product into the row: the batch partial for block-compensated long
+    // rows, else the accumulator.
+    auto fma_step = [&](V a, const vec_t<V, VW>& b) {
+        if constexpr (kBlockComp) {
+            if (long_row) {
+                const float fa = to_f32(a);
+#pragma unroll
+                for (int w = 0; w < VW; ++w) blk[w] = fmaf(fa, to_f32(b.v[w]), blk[w]);
+                return;
+            }
+        }
+        fma_vec(a, b);
+    };
+    auto blk_fold = [&]() {
+        if constexpr (kBlockComp) {
+            if (long_row) {
+#pragma unroll
+                for (int w = 0; w < VW; ++w) acc[w] = comp_add_value(acc[w], blk[w], 0.f);
+            }
+        }
     };
     auto reduce = [&]() {
         if constexpr (NPAR > 1) {
@@ -164,8 +210,10 @@ k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __rest
         }
         if (n_here == UN && row_end - k >= UN) {
             // common case: the batch lies inside the current row
+            blk_zero();
 #pragma unroll
-            for (int u = 0; u < U; ++u) fma_vec(shfl_idx(full, v_cur, bs + u * NPAR, 32), bv[u]);
+            for (int u = 0; u < U; ++u) fma_step(shfl_idx(full, v_cur, bs + u * NPAR, 32), bv[u]);
+            blk_fold();
         } else {
             // segments [s, e) of the batch, one row each, flushed in between
             int s = 0;
@@ -176,12 +224,14 @@ k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __rest
                     continue;
                 }
                 const int ee = e < n_here ? e : n_here;
+                blk_zero();
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const V a = shfl_idx(full, v_cur, (bs + u * NPAR) & 31, 32);
                     const int p = u * NPAR + sub;
-                    if (p >= s && p < ee) fma_vec(a, bv[u]);
+                    if (p >= s && p < ee) fma_step(a, bv[u]);
                 }
+                blk_fold();
                 if (ee == n_here) break;
                 s = ee;
             }
@@ -257,8 +307,9 @@ int launch_seq(const fsb_csr* Am, const V* val, const I* col, const P* ptr, cons
     // Lane vectors of the widest aligned width (whole vectors: n_dense a
     // multiple of the width); otherwise one element per lane.
     constexpr int kMaxVW = seq_max_vw<V, O>();
+    constexpr size_t kCAlign = kMaxVW * sizeof(O) < 16 ? kMaxVW * sizeof(O) : 16;
     const bool wide_ok = ((uintptr_t)B) % (kMaxVW * sizeof(V)) == 0 && ldb % kMaxVW == 0 &&
-                         n_dense % kMaxVW == 0 && ((uintptr_t)C) % (kMaxVW * sizeof(O)) == 0 && ldc % kMaxVW == 0;
+                         n_dense % kMaxVW == 0 && ((uintptr_t)C) % kCAlign == 0 && ldc % kMaxVW == 0;
     const int vw = wide_ok ? kMaxVW : 1;
     // Lanes per nonzero: the column tile (n_tile, or all of n_dense) in lane
     // vectors, rounded up to a power of two, at most 32.
