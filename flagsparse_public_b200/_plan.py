@@ -10,6 +10,7 @@ cached on the prepared object.
 """
 
 import math
+import os
 
 import torch
 
@@ -165,6 +166,66 @@ def default_spmm_plan(stats, n_dense, dtype, row_cap=0):
     if row_cap > 0 or stats.n_rows == 0:
         return KernelPlan(nat.ALGO_ROWS, lanes=32, row_cap=row_cap)
     return KernelPlan(nat.ALGO_SEQ, items_per_unit=seq_items_per_unit(stats))
+
+
+# How the prepared SpMM paths pick their plan: "learned" (the shipped
+# selector network, falling back to autotuning when unsure), "autotune"
+# (time every candidate once per matrix and width) or "heuristic"
+# (default_spmm_plan, no timing).
+PLAN_SELECTORS = ("learned", "autotune", "heuristic")
+_selector_mode = os.environ.get("FSB_PLAN_SELECTOR", "learned")
+_selectors = {}
+_autotuner = None
+
+
+def set_plan_selector(mode):
+    """Select how prepared SpMM calls choose plans (see PLAN_SELECTORS)."""
+    global _selector_mode
+    if mode not in PLAN_SELECTORS:
+        raise ValueError(f"plan selector must be one of {PLAN_SELECTORS}")
+    _selector_mode = mode
+
+
+def plan_selector():
+    return _selector_mode
+
+
+def _tuner():
+    global _autotuner
+    if _autotuner is None:
+        from . import tuning
+        _autotuner = tuning.Autotuner()
+    return _autotuner
+
+
+def learned_selector(device):
+    """The shipped selector on ``device`` (None when no weights are installed)."""
+    from . import tuning
+    key = str(device)
+    sel = _selectors.get(key)
+    if sel is None:
+        if not os.path.exists(tuning.WEIGHTS_PATH):
+            return None
+        sel = tuning.LearnedSelector(device=device, autotuner=_tuner())
+        _selectors[key] = sel
+    return sel
+
+
+def chosen_spmm_plan(stats, data, indices, indptr, n_rows, n_cols, B, C, acc_mode):
+    """Plan for a prepared SpMM call by the current selector mode.  Needs the
+    operands (the learned selector reads the structure on the device, the
+    autotuner runs every candidate into C); not for use inside graph capture."""
+    n_dense = int(B.shape[1])
+    mode = _selector_mode
+    if mode == "heuristic" or stats.n_rows == 0 or n_dense == 0:
+        return default_spmm_plan(stats, n_dense, data.dtype)
+    if mode == "learned":
+        sel = learned_selector(B.device)
+        if sel is not None:
+            return sel.select(data, indices, indptr, n_rows, n_cols, B, C, acc_mode)
+        return default_spmm_plan(stats, n_dense, data.dtype)
+    plan, _ = _tuner().tune(data, indices, indptr, n_rows, n_cols, B, C, acc_mode)
+    return plan
 
 
 def _workspace(is_spmm, cm, n_dense, acc_mode, out_code, cp, device):

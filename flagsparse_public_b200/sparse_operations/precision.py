@@ -64,13 +64,19 @@ def _acc_mode(prepared):
     return _nat.ACC_COMP if prepared.max_row_nnz > prepared.compensate_above else _nat.ACC_NATIVE
 
 
-def _mixed_plan(prepared, kind, n_dense=0):
+def _mixed_plan(prepared, kind, n_dense=0, operands=None):
+    """Cached plan per (kind, width); SpMM plans go through the plan selector
+    when the operands (B, C) are given."""
     key = (kind, int(n_dense))
     plan = prepared._plans.get(key)
     if plan is None:
         st = _stats(prepared)
         if kind == "spmv":
             plan = _plan.default_spmv_plan(st, prepared.data.dtype)
+        elif operands is not None:
+            B, C = operands
+            plan = _plan.chosen_spmm_plan(st, prepared.data, prepared.kernel_indices, prepared.kernel_indptr,
+                                          prepared.n_rows, prepared.n_cols, B, C, _acc_mode(prepared))
         else:
             plan = _plan.default_spmm_plan(st, n_dense, prepared.data.dtype)
         plan.comp_threshold = prepared.compensate_above
@@ -157,7 +163,7 @@ def flagsparse_spmm_csr_mixed(data=None, indices=None, indptr=None, B=None, shap
         t0 = time.perf_counter()
     if prepared.n_rows and n_dense:
         _plan.run_spmm(prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
-                       prepared.n_cols, B, C, _acc_mode(prepared), _mixed_plan(prepared, "spmm", n_dense))
+                       prepared.n_cols, B, C, _acc_mode(prepared), _mixed_plan(prepared, "spmm", n_dense, (B, C)))
     res = [C]
     if return_time:
         torch.cuda.synchronize()

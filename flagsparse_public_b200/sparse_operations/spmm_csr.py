@@ -369,14 +369,21 @@ def prepare_spmm_csr_opt(data, indices, indptr, shape):
     )
 
 
-def _spmm_plan_for(holder, kind, n_dense):
-    """Cached plan on a prepared object for (kind, n_dense)."""
+def _spmm_plan_for(holder, kind, n_dense, operands=None):
+    """Cached plan on a prepared object for (kind, n_dense).  With
+    ``operands`` = (B, C, acc_mode) the first call per width goes through the
+    plan selector (learned / autotune / heuristic); without, the heuristic."""
     key = (kind, int(n_dense))
     plan = holder._plans.get(key)
     if plan is None:
         if holder._stats is None:
             holder._stats = _plan.matrix_stats(holder.kernel_indptr, holder.n_rows, holder.n_cols)
-        plan = _plan.default_spmm_plan(holder._stats, n_dense, holder.data.dtype)
+        if operands is not None and getattr(holder, "kernel_indices", None) is not None:
+            B, C, acc = operands
+            plan = _plan.chosen_spmm_plan(holder._stats, holder.data, holder.kernel_indices, holder.kernel_indptr,
+                                          holder.n_rows, holder.n_cols, B, C, acc)
+        else:
+            plan = _plan.default_spmm_plan(holder._stats, n_dense, holder.data.dtype)
         holder._plans[key] = plan
     return plan
 
@@ -440,7 +447,7 @@ def _triton_spmm_csr_impl_opt_prepared(prepared, B, out=None):
     C = out if out is not None else torch.empty((prepared.n_rows, n_dense), dtype=B.dtype, device=B.device)
     if prepared.n_rows == 0 or n_dense == 0:
         return C.zero_(), False
-    plan = _spmm_plan_for(prepared, "opt", n_dense)
+    plan = _spmm_plan_for(prepared, "opt", n_dense, (B, C, _nat.ACC_NATIVE))
     _plan.run_spmm(prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
                    prepared.n_cols, B, C, _nat.ACC_NATIVE, plan)
     return C, False

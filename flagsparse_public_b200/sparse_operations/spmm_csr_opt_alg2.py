@@ -135,7 +135,7 @@ def _triton_spmm_csr_impl_opt_alg2_prepared(prepared, B, return_meta=False, out=
     C = out if out is not None else torch.empty((prepared.n_rows, n_dense), dtype=B.dtype, device=B.device)
     launch_configs = []
     if prepared.n_rows > 0 and n_dense > 0:
-        plan = _spmm_plan_for(prepared, "alg2", n_dense)
+        plan = _spmm_plan_for(prepared, "alg2", n_dense, (B, C, _nat.ACC_NATIVE))
         _plan.run_spmm(prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
                        prepared.n_cols, B, C, _nat.ACC_NATIVE, plan)
         desc = plan.describe()

@@ -13,6 +13,8 @@ offsets (columns sorted and distinct within a row).  The families:
   4 uniform off-band columns per row, a fraction of rows replaced by long rows
   (precision config: 1,048,576 rows, 1 % of rows with 8192 nonzeros).
 * ``block_diagonal``   -- dense 16 x 16 blocks on the diagonal (BSR family).
+* ``block_sparse``     -- k dense 16 x 16 blocks per block row, the diagonal
+  block among them (BSR family with 16 k nonzeros per row).
 * ``rectangular``      -- random 2:1 rectangular with uniform columns.
 
 Values are U(-1, 1); dense operands N(0, 1).
@@ -157,6 +159,34 @@ def block_diagonal(n_blocks=1024, block=16, seed=0, dtype=torch.bfloat16, device
     pos = torch.arange(nnz, device=device) - indptr[:-1][row_of]
     cols = (row_of // block) * block + pos
     del r
+    data = _uniform_values(g, nnz, dtype, device)
+    return data, cols.to(torch.int32), indptr, (n, n)
+
+
+def block_sparse(n_block_rows=1024, blocks_per_row=2, block=16, seed=0, dtype=torch.float32, device="cuda"):
+    """Square BSR-structured matrix as CSR: each block row holds
+    ``blocks_per_row`` dense ``block`` x ``block`` blocks, the diagonal block
+    and uniform distinct other block columns (sorted)."""
+    g = _gen(seed, device)
+    nb = int(n_block_rows)
+    k = max(1, min(int(blocks_per_row), nb))
+    # block columns per block row: the diagonal plus k - 1 distinct others
+    bcol = torch.empty((nb, k), dtype=torch.int64, device=device)
+    bcol[:, 0] = torch.arange(nb, device=device)
+    if k > 1:
+        brow_of = torch.repeat_interleave(torch.arange(nb, device=device), k - 1)
+        lens = torch.full((nb,), k - 1, dtype=torch.int64, device=device)
+        others = _distinct_sorted_columns(g, brow_of, lens, max(nb - 1, 1), device)
+        others = others.view(nb, k - 1)
+        others = torch.where(others >= torch.arange(nb, device=device)[:, None], others + 1, others)
+        bcol[:, 1:] = others
+    bcol, _ = torch.sort(bcol, dim=1)
+    n = nb * block
+    lengths = torch.full((n,), k * block, dtype=torch.int64, device=device)
+    indptr, row_of, nnz = _rows_from_lengths(lengths, device)
+    pos = torch.arange(nnz, device=device) - indptr[:-1][row_of]
+    br = row_of // block
+    cols = bcol[br, pos // block] * block + pos % block
     data = _uniform_values(g, nnz, dtype, device)
     return data, cols.to(torch.int32), indptr, (n, n)
 

@@ -188,6 +188,50 @@ int fsb_spmm_coo_atomic(const void* values, const void* row, const void* col,
                         const void* B, int64_t ldb, int64_t n_dense, void* C,
                         int64_t ldc, int acc_dtype, void* stream);
 
+/* ---- learned plan selector -------------------------------------------- *
+ * No FlagSparse counterpart: FlagSparse picks its launch parameters by
+ * fixed row-length buckets and device-property heuristics
+ * (spmm_csr.py:395-414, spmm_csr_opt_alg2.py:175-304).  These entry points
+ * are the device side of the learned selector that replaces them.         */
+
+/* Structure features of a CSR matrix (five doubles, written on stream):
+ * out[0] = sum of row lengths, out[1] = sum of squared row lengths,
+ * out[2] = longest row (an unsigned 64-bit integer held in the slot's bits),
+ * out[3] = empty rows, out[4] = sum over nonzeros of
+ * |col - r * n_cols / n_rows| / n_cols.  Sums of doubles are accumulated
+ * with atomics (last-bit order dependence).                               */
+int fsb_csr_features(const void* row_ptr, int ptr_dtype, const void* col_idx,
+                     int index_dtype, int64_t n_rows, int64_t n_cols,
+                     double* out, void* stream);
+
+/* The selector network: d_in -> h1 (ReLU) -> h2 (ReLU) -> d_out, float32,
+ * parameters packed W1[d_in][h1], b1, W2[h1][h2], b2, W3[h2][d_out], b3
+ * (d_in <= 16, h1, h2 <= 64, d_out <= 32).  Returns the parameter count.  */
+int fsb_mlp_param_count(int d_in, int h1, int h2, int d_out);
+
+/* Y[n][d_out] = network(X[n][d_in]).  cache (may be null) receives per
+ * sample the pre-activations Z1[h1], Z2[h2] and Y[d_out].                 */
+int fsb_mlp_forward(const float* X, int n, int d_in, int h1, int h2,
+                    int d_out, const float* params, float* Y, float* cache,
+                    void* stream);
+
+/* Gradient of L = inv_terms * sum mask (Y - T)^2 with respect to the
+ * parameters, from a forward cache: grad (packed like params) is written
+ * with fixed-order sums over the samples; loss_terms[n] receives each
+ * sample's sum of masked squared errors; deltas is n x (h1 + h2 + d_out)
+ * scratch.                                                                 */
+int fsb_mlp_backward(const float* X, int n, int d_in, int h1, int h2,
+                     int d_out, const float* params, const float* cache,
+                     const float* targets, const float* mask, float inv_terms,
+                     float* deltas, float* loss_terms, float* grad,
+                     void* stream);
+
+/* One Adam step (Kingma & Ba, bias-corrected, step >= 1); weight_decay
+ * adds weight_decay * p to the gradient (L2 regularisation).              */
+int fsb_adam_step(float* params, const float* grad, float* m1, float* m2,
+                  int n_params, float lr, float beta1, float beta2, float eps,
+                  int step, float weight_decay, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
