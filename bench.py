@@ -25,6 +25,7 @@ device, max over ranks.
 
 import argparse
 import json
+import math
 import os
 import statistics
 import sys
@@ -481,6 +482,12 @@ class PrecisionBanded:
 
         fs.flagsparse_spmm_csr_opt(B=self.B, prepared=self.p32mm, out=self.C)
 
+    def speedups(self, extra, ms_step, plain_ms):
+        out = {"speedup_spmm_bf16_vs_f32": plain_ms / ms_step}
+        if "spmv_bf16" in extra:
+            out["speedup_spmv_bf16_vs_f32"] = extra["spmv_f32_fp32acc"]["ms_per_step"] / extra["spmv_bf16"]["ms_per_step"]
+        return out
+
     def extra_forms(self):
         import flagsparse_public_b200 as fs
 
@@ -561,7 +568,139 @@ class PrecisionBanded:
         return run, nbytes, f"rows [0, {rows}) ({k} nonzeros), bf16 inputs, f32 accumulation, N = {self.n_dense}"
 
 
-WORKLOADS = {"spmm_powerlaw": SpmmPowerlaw, "spmv_poisson": SpmvPoisson, "precision_banded": PrecisionBanded}
+class BatchedUneven:
+    """512 independent square CSR matrices, rows log-uniform in [1024, 65536],
+    Poisson row lengths with mean U[2, 64] per matrix, fp32 values, int32
+    indices, each times its own 32-column N(0, 1) operand.  Chosen form: the
+    batch stacked block-diagonally, one persistent launch of the batched
+    merge-path kernel (plan from the autotuner) replayed from a CUDA graph.
+    Plain form: FlagSparse's way, one flagsparse_spmm_csr call per matrix."""
+
+    metric = "batched uneven CSR SpMM useful throughput (512 matrices, one graph launch)"
+    unit = "GB/s"
+    graph_iters = 1  # one captured launch pair per step
+    n_mats = 512
+    n_dense = 32
+
+    def specs(self):
+        import numpy as np
+
+        rng = np.random.default_rng(0)
+        out = []
+        for i in range(self.n_mats):
+            n = int(round(math.exp(rng.uniform(math.log(1024), math.log(65536)))))
+            out.append((n, float(rng.uniform(2.0, 64.0)), int(rng.integers(1 << 30))))
+        return out
+
+    def generate(self, device):
+        from flagsparse_public_b200 import synthetic
+
+        self.mats = [synthetic.poisson_uniform(n, n, mean=m, seed=s, device=device) for n, m, s in self.specs()]
+        self.nnz = sum(int(m[0].numel()) for m in self.mats)
+        self.rows = sum(int(m[3][0]) for m in self.mats)
+        self.useful_bytes = self.nnz * 8 + 2 * self.rows * self.n_dense * 4
+        self.flops = 2 * self.nnz * self.n_dense
+
+    def build(self, device):
+        from flagsparse_public_b200 import batched, synthetic
+
+        self.generate(device)
+        self.prep = batched.prepare_spmm_csr_batch(self.mats, self.n_dense)
+        self.prep.B.copy_(synthetic.dense_operand(self.prep.n_cols, self.n_dense, seed=1, device=device))
+        self.prep.capture()
+        self.plain_C = [torch.empty_like(c) for c in self.prep.c_views]
+        self.seq_plans = [self.prep.plan.copy() for _ in self.mats]
+
+    def config(self):
+        return {"workload": "csr_spmm_batched512_rows1024to65536_poisson2to64_n32_f32_i32",
+                "matrices": self.n_mats, "n_rows_total": self.rows, "nnz": self.nnz, "n_dense": self.n_dense,
+                "global_batch": self.n_mats, "parallelism": "replicas",
+                "l2": "inputs larger than L2 (4.3 GB); flushed before every timed step (256 MiB write)",
+                "autotune_ms": self.prep.timings}
+
+    def step(self):
+        self.prep.graph.replay()
+
+    plain_desc = "512 sequential flagsparse_spmm_csr calls (float64 accumulation, FlagSparse plain)"
+
+    def plain_step(self):
+        import flagsparse_public_b200 as fs
+
+        for m, b, c in zip(self.mats, self.prep.b_views, self.plain_C):
+            fs.flagsparse_spmm_csr(m[0], m[1], m[2], b, m[3], out=c)
+
+    def _seq_each(self):
+        from flagsparse_public_b200 import _plan
+
+        for m, b, c, p in zip(self.mats, self.prep.b_views, self.plain_C, self.seq_plans):
+            _plan.run_spmm(m[0], m[1], m[2], m[3][0], m[3][1], b, c, 0, p)
+
+    def extra_forms(self):
+        return {"sequential_batched_kernel": (self._seq_each, self.useful_bytes)}
+
+    def speedups(self, extra, ms_step, plain_ms):
+        return {"speedup_vs_sequential_plain": plain_ms / ms_step,
+                "speedup_vs_sequential_same_kernel": extra["sequential_batched_kernel"]["ms_per_step"] / ms_step}
+
+    def plan_desc(self):
+        return self.prep.plan.describe()
+
+    def force_plan(self, plan):
+        from flagsparse_public_b200 import batched
+
+        self.prep = batched.prepare_spmm_csr_batch(self.mats, self.n_dense, plan=plan)
+        self.prep.B.normal_()
+        self.prep.capture()
+
+    def host_inputs(self):
+        self.h_B = self.prep.B.cpu().pin_memory()
+        self.h_C = torch.empty(self.prep.C.shape, dtype=self.prep.C.dtype).pin_memory()
+        self.h2d_bytes = self.h_B.numel() * self.h_B.element_size()
+        self.d2h_bytes = self.h_C.numel() * self.h_C.element_size()
+
+    e2e_what = ("matrices prepared once (resident); per step every dense operand pinned host -> device, "
+                "one batch product, every result -> pinned host")
+
+    def e2e_step(self, device):
+        # the matrices are prepared once; each step moves every dense operand
+        # in and every product out through the prepared batch
+        self.prep.B.copy_(self.h_B, non_blocking=True)
+        self.prep.run()
+        self.h_C.copy_(self.prep.C, non_blocking=True)
+
+    def fp64_error(self):
+        from oracle import oracle as orc
+        from tests.numerics import scaled_error
+
+        self.prep.run()
+        self.plain_step()
+        torch.cuda.synchronize()
+        worst = {"chosen": 0.0, "plain": 0.0}
+        for i in range(0, self.n_mats, 32):  # every 32nd matrix
+            m = self.mats[i]
+            data, indices, indptr = (t.cpu() for t in m[:3])
+            exact, mag = orc.spmm_csr_exact(data, indices, indptr, self.prep.b_views[i].cpu())
+            worst["chosen"] = max(worst["chosen"], scaled_error(self.prep.c_views[i], exact, mag))
+            worst["plain"] = max(worst["plain"], scaled_error(self.plain_C[i], exact, mag))
+        worst["definition"] = "max |c - c64| / sum_k |a_k b_k| over every 32nd matrix"
+        return worst
+
+    def cpu_step_factory(self, threads, sample_rows=None):
+        from oracle import oracle as orc
+
+        picks = list(range(0, self.n_mats, 16))  # every 16th matrix
+        host = [(tuple(t.cpu() for t in self.mats[i][:3]), self.prep.b_views[i].cpu()) for i in picks]
+        nbytes = sum(a[0].numel() * 8 + 2 * b.shape[0] * self.n_dense * 4 for a, b in host)
+
+        def run():
+            for (data, indices, indptr), b in host:
+                orc.spmm_csr(data, indices, indptr, b, acc_mode=orc.ACC_NATIVE, threads=threads)
+
+        return run, nbytes, f"every 16th matrix ({len(picks)} of {self.n_mats}), N = {self.n_dense}"
+
+
+WORKLOADS = {"spmm_powerlaw": SpmmPowerlaw, "spmv_poisson": SpmvPoisson, "precision_banded": PrecisionBanded,
+             "batched_uneven": BatchedUneven}
 
 
 # ------------------------------------------------------------------ timing --
@@ -691,9 +830,7 @@ def run_ours(args):
             torch.cuda.synchronize()
             ms_x = max_over_ranks(sum(time_device_steps(fn, args.steps, flush)), world) / args.steps
             extra[name] = {"ms_per_step": ms_x, "value": nbytes * world / (ms_x * 1e-3) / 1e9, "unit": wl.unit}
-        extra["speedup_spmm_bf16_vs_f32"] = plain_ms / ms_step
-        if "spmv_bf16" in extra:
-            extra["speedup_spmv_bf16_vs_f32"] = extra["spmv_f32_fp32acc"]["ms_per_step"] / extra["spmv_bf16"]["ms_per_step"]
+        extra.update(wl.speedups(extra, ms_step, plain_ms))
 
     e2e = None
     if not args.no_e2e:
@@ -713,8 +850,8 @@ def run_ours(args):
         per_step_bytes = wl.useful_bytes / getattr(wl, "graph_iters", 1)
         e2e = {"value": per_step_bytes * world / (e_ms * 1e-3) / 1e9, "unit": wl.unit, "ms_per_step": e_ms,
                "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes,
-               "what": "pinned host A and dense operand -> device, public one-shot API (prepare + product), "
-                       "result -> pinned host"}
+               "what": getattr(wl, "e2e_what", "pinned host A and dense operand -> device, public one-shot API "
+                                               "(prepare + product), result -> pinned host")}
 
     errors = wl.fp64_error() if rank == 0 else None
 

@@ -64,10 +64,10 @@ class KernelPlan:
     """One launch configuration of fsb_spmv_csr / fsb_spmm_csr."""
 
     __slots__ = ("algo", "lanes", "items_per_unit", "n_tile", "snap", "coords", "n_units", "row_cap",
-                 "comp_threshold", "fallback_ok")
+                 "comp_threshold", "fallback_ok", "grid_blocks")
 
     def __init__(self, algo, lanes=32, items_per_unit=0, n_tile=0, snap=0, row_cap=0, comp_threshold=0,
-                 fallback_ok=False):
+                 fallback_ok=False, grid_blocks=0):
         self.algo = int(algo)
         self.lanes = int(lanes)
         self.items_per_unit = int(items_per_unit)
@@ -78,6 +78,7 @@ class KernelPlan:
         self.row_cap = int(row_cap)
         self.comp_threshold = int(comp_threshold)
         self.fallback_ok = bool(fallback_ok)
+        self.grid_blocks = int(grid_blocks)
 
     def as_flat(self):
         """The register-staged flat plan over the same merge-path units."""
@@ -87,7 +88,7 @@ class KernelPlan:
         return p
 
     def key(self):
-        return (self.algo, self.lanes, self.items_per_unit, self.n_tile, self.snap)
+        return (self.algo, self.lanes, self.items_per_unit, self.n_tile, self.snap, self.grid_blocks)
 
     def describe(self):
         if self.algo == nat.ALGO_ROWS:
@@ -95,12 +96,15 @@ class KernelPlan:
             return {"kind": kind, "lanes": self.lanes, "n_tile": self.n_tile}
         kind = {nat.ALGO_MERGE: "merge_path", nat.ALGO_FLAT: "merge_path_flat",
                 nat.ALGO_GATHER: "merge_path_tma_gather", nat.ALGO_SEQ: "merge_path_seq"}[self.algo]
-        return {"kind": kind, "items_per_unit": self.items_per_unit, "n_tile": self.n_tile,
-                "snap": self.snap, "n_units": self.n_units}
+        d = {"kind": kind, "items_per_unit": self.items_per_unit, "n_tile": self.n_tile,
+             "snap": self.snap, "n_units": self.n_units}
+        if self.grid_blocks:
+            d["grid_blocks"] = self.grid_blocks
+        return d
 
     def copy(self):
         p = KernelPlan(self.algo, self.lanes, self.items_per_unit, self.n_tile, self.snap, self.row_cap,
-                       self.comp_threshold, self.fallback_ok)
+                       self.comp_threshold, self.fallback_ok, self.grid_blocks)
         return p
 
     def ensure_coords(self, row_ptr, n_rows, nnz):
@@ -121,7 +125,7 @@ class KernelPlan:
     def c_plan(self):
         return nat.make_plan(self.algo, lanes=self.lanes, items_per_unit=self.items_per_unit, n_tile=self.n_tile,
                              coords=self.coords, n_units=self.n_units, row_cap=self.row_cap,
-                             comp_threshold=self.comp_threshold)
+                             comp_threshold=self.comp_threshold, grid_blocks=self.grid_blocks)
 
 
 def _pow2_clamp(v, lo, hi):

@@ -62,206 +62,210 @@ k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __rest
     constexpr bool kBlockComp = is_comp_acc<A>::value && sizeof(V) == 2;
     constexpr int UN = U * NPAR;  // nonzeros per batch (divides 32)
     const int lane = threadIdx.x & 31;
-    const int64_t unit = (int64_t)blockIdx.x * (kSpmmThreads / 32) + (threadIdx.x >> 5);
-    if (unit >= n_units) return;  // whole warp
-    const unsigned full = 0xffffffffu;
-    const int sub = lane >> LPN_LOG2;
-    const int64_t c0 = (int64_t)blockIdx.y * (LPN * VW) + (int64_t)(lane & (LPN - 1)) * VW;
-    const bool col_ok = c0 < n_dense;
-    // lanes past the last column read column 0 (a valid address) and store nothing
-    const V* Bl = B + (col_ok ? c0 : 0);
-    const uint64_t keep_b = policy_evict_last();
+    // Persistent when the grid is smaller than the unit count: each warp
+    // takes units warp_id, warp_id + total warps, ...
+    const int64_t unit_stride = (int64_t)gridDim.x * (kSpmmThreads / 32);
+    for (int64_t unit = (int64_t)blockIdx.x * (kSpmmThreads / 32) + (threadIdx.x >> 5); unit < n_units;
+         unit += unit_stride) {  // whole warp
+        const unsigned full = 0xffffffffu;
+        const int sub = lane >> LPN_LOG2;
+        const int64_t c0 = (int64_t)blockIdx.y * (LPN * VW) + (int64_t)(lane & (LPN - 1)) * VW;
+        const bool col_ok = c0 < n_dense;
+        // lanes past the last column read column 0 (a valid address) and store nothing
+        const V* Bl = B + (col_ok ? c0 : 0);
+        const uint64_t keep_b = policy_evict_last();
 
-    const int64_t r0 = coords[2 * unit], k0 = coords[2 * unit + 1];
-    const int64_t r1 = coords[2 * unit + 2], k1 = coords[2 * unit + 3];
-    const int64_t last_row = r1 < n_rows ? r1 : r1 - 1;
-    const int nk = (int)(k1 - k0);  // unit nonzeros (the host keeps units far below 2^31)
+        const int64_t r0 = coords[2 * unit], k0 = coords[2 * unit + 1];
+        const int64_t r1 = coords[2 * unit + 2], k1 = coords[2 * unit + 3];
+        const int64_t last_row = r1 < n_rows ? r1 : r1 - 1;
+        const int nk = (int)(k1 - k0);  // unit nonzeros (the host keeps units far below 2^31)
 
-    // Row ends relative to k0; a row ending past the unit reads as kNoEnd.
-    auto load_ends = [&](int64_t rbase) -> int {
-        const int64_t r = rbase + lane;
-        if (r > last_row) return kNoEnd;
-        const int64_t e = idx(ptr[r + 1]) - k0;
-        return e > (int64_t)kNoEnd ? kNoEnd : (int)e;
-    };
-    // rows rb .. rb + 31 in e_win, the next 32 prefetched in e_nxt
-    int64_t rb = r0;
-    int e_win = load_ends(rb);
-    int e_nxt = load_ends(rb + 32);
-    int64_t row = r0;
-    int64_t row_start = (r0 < n_rows) ? idx(ptr[r0]) : k0;  // global start of the current row
-    const bool continued = (r0 < n_rows) && (k0 > row_start);
-    int row_end = __shfl_sync(full, e_win, 0);
-    // FSB_ACC_COMP: compensated accumulation only on rows longer than
-    // comp_threshold nonzeros; shorter rows add plainly into the f32 part.
-    auto row_is_long = [&]() -> bool {
-        if constexpr (!is_comp_acc<A>::value) return false;
-        if (row > last_row) return false;
-        const int64_t len = (row_end == kNoEnd ? idx(ptr[row + 1]) : k0 + row_end) - row_start;
-        return len > comp_threshold;
-    };
-    bool long_row = row_is_long();
+        // Row ends relative to k0; a row ending past the unit reads as kNoEnd.
+        auto load_ends = [&](int64_t rbase) -> int {
+            const int64_t r = rbase + lane;
+            if (r > last_row) return kNoEnd;
+            const int64_t e = idx(ptr[r + 1]) - k0;
+            return e > (int64_t)kNoEnd ? kNoEnd : (int)e;
+        };
+        // rows rb .. rb + 31 in e_win, the next 32 prefetched in e_nxt
+        int64_t rb = r0;
+        int e_win = load_ends(rb);
+        int e_nxt = load_ends(rb + 32);
+        int64_t row = r0;
+        int64_t row_start = (r0 < n_rows) ? idx(ptr[r0]) : k0;  // global start of the current row
+        const bool continued = (r0 < n_rows) && (k0 > row_start);
+        int row_end = __shfl_sync(full, e_win, 0);
+        // FSB_ACC_COMP: compensated accumulation only on rows longer than
+        // comp_threshold nonzeros; shorter rows add plainly into the f32 part.
+        auto row_is_long = [&]() -> bool {
+            if constexpr (!is_comp_acc<A>::value) return false;
+            if (row > last_row) return false;
+            const int64_t len = (row_end == kNoEnd ? idx(ptr[row + 1]) : k0 + row_end) - row_start;
+            return len > comp_threshold;
+        };
+        bool long_row = row_is_long();
 
-    A acc[VW];
-    zero_acc<A, VW>(acc);
-    auto fma_vec = [&](V a, const vec_t<V, VW>& b) {
-        if constexpr (is_comp_acc<A>::value) {
-            if (!long_row) {
-#pragma unroll
-                for (int w = 0; w < VW; ++w) acc[w].s = fmaf(to_f32(a), to_f32(b.v[w]), acc[w].s);
-                return;
-            }
-        }
-#pragma unroll
-        for (int w = 0; w < VW; ++w) acc[w] = Acc<V, A>::fma(a, b.v[w], acc[w]);
-    };
-    // Per-batch partial sums of the block-compensated rows.
-    float blk[kBlockComp ? VW : 1];
-    auto blk_zero = [&]() {
-        if constexpr (kBlockComp) {
-#pragma unroll
-            for (int w = 0; w < VW; ++w) blk[w] = 0.f;
-        }
-    };
-    // One product into the row: the batch partial for block-compensated long
-    // rows, else the accumulator.
-    auto fma_step = [&](V a, const vec_t<V, VW>& b) {
-        if constexpr (kBlockComp) {
-            if (long_row) {
-                const float fa = to_f32(a);
-#pragma unroll
-                for (int w = 0; w < VW; ++w) blk[w] = fmaf(fa, to_f32(b.v[w]), blk[w]);
-                return;
-            }
-        }
-        fma_vec(a, b);
-    };
-    auto blk_fold = [&]() {
-        if constexpr (kBlockComp) {
-            if (long_row) {
-#pragma unroll
-                for (int w = 0; w < VW; ++w) acc[w] = comp_add_value(acc[w], blk[w], 0.f);
-            }
-        }
-    };
-    auto reduce = [&]() {
-        if constexpr (NPAR > 1) {
-#pragma unroll
-            for (int w = 0; w < VW; ++w) acc[w] = segment_reduce(full, acc[w], LPN, 32);
-        }
-    };
-    // Store the finished current row and move to the next one.
-    auto flush = [&]() {
-        reduce();
-        if (sub == 0 && col_ok) {
-            if (row == r0 && continued) {
-                A* dst = head_val + unit * n_dense + c0;
-#pragma unroll
-                for (int w = 0; w < VW; ++w) dst[w] = acc[w];
-            } else {
-                const int64_t out_row = row_map ? idx(row_map[row_start]) : row;
-                store_row<O, A, VW>(C, ldc, out_row, c0, acc);
-            }
-        }
+        A acc[VW];
         zero_acc<A, VW>(acc);
-        ++row;
-        row_start = k0 + row_end;
-        if (row <= last_row && row - rb >= 32) {
-            rb += 32;
-            e_win = e_nxt;
-            e_nxt = load_ends(rb + 32);
-        }
-        row_end = row <= last_row ? __shfl_sync(full, e_win, (int)(row - rb)) : kNoEnd;
-        long_row = row_is_long();
-    };
-    auto b_row = [&](I c) -> const V* {
-        if constexpr (ADDR32) return Bl + (uint32_t)((uint32_t)c * (uint32_t)ldb);
-        else return Bl + idx(c) * ldb;
-    };
-
-    // Value / column windows: lane l holds entry kb + l (current) and
-    // kb + 32 + l (next), relative to k0.
-    int kb = 0;
-    V v_cur = vzero<V>(), v_nxt = vzero<V>();
-    I c_cur = 0, c_nxt = 0;
-    if (lane < nk) { v_cur = ld_stream1(val + k0 + lane); c_cur = ld_stream1(col + k0 + lane); }
-    if (32 + lane < nk) { v_nxt = ld_stream1(val + k0 + 32 + lane); c_nxt = ld_stream1(col + k0 + 32 + lane); }
-
-    for (int k = 0; k < nk;) {
-        // UN divides 32 and k advances by UN except at the unit end, so a batch
-        // never crosses the window: bs + u * NPAR stays below 32
-        const int n_here = nk - k < UN ? nk - k : UN;
-        const int bs = (k - kb) + sub;
-        vec_t<V, VW> bv[U];
-        if (n_here == UN) {
+        auto fma_vec = [&](V a, const vec_t<V, VW>& b) {
+            if constexpr (is_comp_acc<A>::value) {
+                if (!long_row) {
 #pragma unroll
-            for (int u = 0; u < U; ++u) bv[u] = ld_keep<V, VW>(b_row(shfl_idx(full, c_cur, bs + u * NPAR, 32)), keep_b);
-        } else {
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const I c = shfl_idx(full, c_cur, (bs + u * NPAR) & 31, 32);
-                if (u * NPAR + sub < n_here) {
-                    bv[u] = ld_keep<V, VW>(b_row(c), keep_b);
-                } else {
-#pragma unroll
-                    for (int w = 0; w < VW; ++w) bv[u].v[w] = vzero<V>();
+                    for (int w = 0; w < VW; ++w) acc[w].s = fmaf(to_f32(a), to_f32(b.v[w]), acc[w].s);
+                    return;
                 }
             }
-        }
-        if (n_here == UN && row_end - k >= UN) {
-            // common case: the batch lies inside the current row
-            blk_zero();
 #pragma unroll
-            for (int u = 0; u < U; ++u) fma_step(shfl_idx(full, v_cur, bs + u * NPAR, 32), bv[u]);
-            blk_fold();
-        } else {
-            // segments [s, e) of the batch, one row each, flushed in between
-            int s = 0;
-            for (;;) {
-                const int e = row_end - k;
-                if (e <= s) {
-                    flush();
-                    continue;
-                }
-                const int ee = e < n_here ? e : n_here;
-                blk_zero();
+            for (int w = 0; w < VW; ++w) acc[w] = Acc<V, A>::fma(a, b.v[w], acc[w]);
+        };
+        // Per-batch partial sums of the block-compensated rows.
+        float blk[kBlockComp ? VW : 1];
+        auto blk_zero = [&]() {
+            if constexpr (kBlockComp) {
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const V a = shfl_idx(full, v_cur, (bs + u * NPAR) & 31, 32);
-                    const int p = u * NPAR + sub;
-                    if (p >= s && p < ee) fma_step(a, bv[u]);
+                for (int w = 0; w < VW; ++w) blk[w] = 0.f;
+            }
+        };
+        // One product into the row: the batch partial for block-compensated long
+        // rows, else the accumulator.
+        auto fma_step = [&](V a, const vec_t<V, VW>& b) {
+            if constexpr (kBlockComp) {
+                if (long_row) {
+                    const float fa = to_f32(a);
+#pragma unroll
+                    for (int w = 0; w < VW; ++w) blk[w] = fmaf(fa, to_f32(b.v[w]), blk[w]);
+                    return;
                 }
-                blk_fold();
-                if (ee == n_here) break;
-                s = ee;
             }
-        }
-        k += n_here;
-        if (k - kb == 32) {
-            kb += 32;
-            v_cur = v_nxt;
-            c_cur = c_nxt;
-            if (kb + 32 + lane < nk) {
-                v_nxt = ld_stream1(val + k0 + kb + 32 + lane);
-                c_nxt = ld_stream1(col + k0 + kb + 32 + lane);
+            fma_vec(a, b);
+        };
+        auto blk_fold = [&]() {
+            if constexpr (kBlockComp) {
+                if (long_row) {
+#pragma unroll
+                    for (int w = 0; w < VW; ++w) acc[w] = comp_add_value(acc[w], blk[w], 0.f);
+                }
             }
-        }
-    }
-    while (row < r1) flush();  // rows ending at the unit end, empty rows
-    bool open = false;
-    if (r1 < n_rows) {
-        const int64_t s1 = row_start > k0 ? row_start : k0;  // row == r1 here
-        open = k1 > s1;
-        if (open) {
+        };
+        auto reduce = [&]() {
+            if constexpr (NPAR > 1) {
+#pragma unroll
+                for (int w = 0; w < VW; ++w) acc[w] = segment_reduce(full, acc[w], LPN, 32);
+            }
+        };
+        // Store the finished current row and move to the next one.
+        auto flush = [&]() {
             reduce();
             if (sub == 0 && col_ok) {
-                A* dst = carry_val + unit * n_dense + c0;
+                if (row == r0 && continued) {
+                    A* dst = head_val + unit * n_dense + c0;
 #pragma unroll
-                for (int w = 0; w < VW; ++w) dst[w] = acc[w];
+                    for (int w = 0; w < VW; ++w) dst[w] = acc[w];
+                } else {
+                    const int64_t out_row = row_map ? idx(row_map[row_start]) : row;
+                    store_row<O, A, VW>(C, ldc, out_row, c0, acc);
+                }
+            }
+            zero_acc<A, VW>(acc);
+            ++row;
+            row_start = k0 + row_end;
+            if (row <= last_row && row - rb >= 32) {
+                rb += 32;
+                e_win = e_nxt;
+                e_nxt = load_ends(rb + 32);
+            }
+            row_end = row <= last_row ? __shfl_sync(full, e_win, (int)(row - rb)) : kNoEnd;
+            long_row = row_is_long();
+        };
+        auto b_row = [&](I c) -> const V* {
+            if constexpr (ADDR32) return Bl + (uint32_t)((uint32_t)c * (uint32_t)ldb);
+            else return Bl + idx(c) * ldb;
+        };
+
+        // Value / column windows: lane l holds entry kb + l (current) and
+        // kb + 32 + l (next), relative to k0.
+        int kb = 0;
+        V v_cur = vzero<V>(), v_nxt = vzero<V>();
+        I c_cur = 0, c_nxt = 0;
+        if (lane < nk) { v_cur = ld_stream1(val + k0 + lane); c_cur = ld_stream1(col + k0 + lane); }
+        if (32 + lane < nk) { v_nxt = ld_stream1(val + k0 + 32 + lane); c_nxt = ld_stream1(col + k0 + 32 + lane); }
+
+        for (int k = 0; k < nk;) {
+            // UN divides 32 and k advances by UN except at the unit end, so a batch
+            // never crosses the window: bs + u * NPAR stays below 32
+            const int n_here = nk - k < UN ? nk - k : UN;
+            const int bs = (k - kb) + sub;
+            vec_t<V, VW> bv[U];
+            if (n_here == UN) {
+#pragma unroll
+                for (int u = 0; u < U; ++u) bv[u] = ld_keep<V, VW>(b_row(shfl_idx(full, c_cur, bs + u * NPAR, 32)), keep_b);
+            } else {
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const I c = shfl_idx(full, c_cur, (bs + u * NPAR) & 31, 32);
+                    if (u * NPAR + sub < n_here) {
+                        bv[u] = ld_keep<V, VW>(b_row(c), keep_b);
+                    } else {
+#pragma unroll
+                        for (int w = 0; w < VW; ++w) bv[u].v[w] = vzero<V>();
+                    }
+                }
+            }
+            if (n_here == UN && row_end - k >= UN) {
+                // common case: the batch lies inside the current row
+                blk_zero();
+#pragma unroll
+                for (int u = 0; u < U; ++u) fma_step(shfl_idx(full, v_cur, bs + u * NPAR, 32), bv[u]);
+                blk_fold();
+            } else {
+                // segments [s, e) of the batch, one row each, flushed in between
+                int s = 0;
+                for (;;) {
+                    const int e = row_end - k;
+                    if (e <= s) {
+                        flush();
+                        continue;
+                    }
+                    const int ee = e < n_here ? e : n_here;
+                    blk_zero();
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const V a = shfl_idx(full, v_cur, (bs + u * NPAR) & 31, 32);
+                        const int p = u * NPAR + sub;
+                        if (p >= s && p < ee) fma_step(a, bv[u]);
+                    }
+                    blk_fold();
+                    if (ee == n_here) break;
+                    s = ee;
+                }
+            }
+            k += n_here;
+            if (k - kb == 32) {
+                kb += 32;
+                v_cur = v_nxt;
+                c_cur = c_nxt;
+                if (kb + 32 + lane < nk) {
+                    v_nxt = ld_stream1(val + k0 + kb + 32 + lane);
+                    c_nxt = ld_stream1(col + k0 + kb + 32 + lane);
+                }
             }
         }
+        while (row < r1) flush();  // rows ending at the unit end, empty rows
+        bool open = false;
+        if (r1 < n_rows) {
+            const int64_t s1 = row_start > k0 ? row_start : k0;  // row == r1 here
+            open = k1 > s1;
+            if (open) {
+                reduce();
+                if (sub == 0 && col_ok) {
+                    A* dst = carry_val + unit * n_dense + c0;
+#pragma unroll
+                    for (int w = 0; w < VW; ++w) dst[w] = acc[w];
+                }
+            }
+        }
+        if (blockIdx.y == 0 && lane == 0) carry_row[unit] = open ? r1 : -1;
     }
-    if (blockIdx.y == 0 && lane == 0) carry_row[unit] = open ? r1 : -1;
 }
 
 // Widest lane vector: 16 bytes of B and of C.
@@ -333,7 +337,10 @@ int launch_seq(const fsb_csr* Am, const V* val, const I* col, const P* ptr, cons
     A* cv = static_cast<A*>(ms.carry_val);
     A* hv = static_cast<A*>(ms.head_val);
     const int64_t thr = plan->comp_threshold > 0 ? plan->comp_threshold : 0;
-    dim3 g((unsigned)blocks, (unsigned)col_tiles);
+    // plan->grid_blocks > 0: a persistent grid of that many CTAs per column
+    // tile, its warps striding over the units
+    const int64_t grid = plan->grid_blocks > 0 && plan->grid_blocks < blocks ? plan->grid_blocks : blocks;
+    dim3 g((unsigned)grid, (unsigned)col_tiles);
     if (vw == kMaxVW)
         launch_seq_vw<V, A, O, I, P, kMaxVW>(lpn_log2, addr32, g, st, val, col, ptr, rmap, B, ldb, C, ldc, Am->n_rows,
                                              n_dense, plan->unit_coords, n_units, thr, ms.carry_row, cv, hv);

@@ -140,15 +140,16 @@ def _time_ms(fn, reps):
 def time_candidates(data, indices, indptr, n_rows, n_cols, B, C, acc_mode, candidates=SPMM_CANDIDATES, reps=3,
                     slow_ms=5.0):
     """Milliseconds per call of each candidate plan (inf where a plan cannot
-    run these operands).  One untimed call first (partition, first touch),
-    then ``reps`` timed calls (one when the untimed call took > slow_ms)."""
+    run these operands).  One untimed call first (partition, workspace, first
+    touch), then ``reps`` timed calls (one when a call takes > slow_ms)."""
     times = []
     for _name, make in candidates:
         plan = make()
         run = lambda: _plan.run_spmm(data, indices, indptr, n_rows, n_cols, B, C, acc_mode, plan)  # noqa: E731
         try:
-            t0 = _time_ms(run, 1)
-            times.append(t0 if t0 > slow_ms else _time_ms(run, reps))
+            _time_ms(run, 1)  # untimed: one-time costs
+            t1 = _time_ms(run, 1)
+            times.append(t1 if t1 > slow_ms or reps <= 1 else _time_ms(run, reps))
         except (RuntimeError, ValueError):
             times.append(float("inf"))
     return times

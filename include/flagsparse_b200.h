@@ -100,7 +100,8 @@ typedef struct fsb_plan {
                                 (FlagSparse max_segments * block_nnz)             */
     int64_t comp_threshold;  /* FSB_ACC_COMP: rows longer than this are
                                 compensated (FlagSparse precision form: 4096)     */
-    int32_t grid_blocks;     /* ROWS: CTAs to launch, 0 = automatic                */
+    int32_t grid_blocks;     /* ROWS, SEQ: CTAs to launch (SEQ: a persistent grid
+                                striding over the units), 0 = automatic           */
     int32_t flags;           /* reserved, 0                                         */
 } fsb_plan;
 

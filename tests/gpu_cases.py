@@ -68,6 +68,8 @@ def spmm_plans():
               for ipu, snap, nt in ((16, 0, 0), (100, 0, 0), (256, 128, 0), (2048, 0, 0), (128, 64, 32), (64, 0, 0))]
     plans += [_plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=ipu, snap=snap, n_tile=nt)
               for ipu, snap, nt in ((16, 0, 0), (100, 0, 0), (256, 128, 0), (2048, 0, 0), (128, 64, 32), (77, 0, 8))]
+    # persistent grids: one and three CTAs striding over every unit
+    plans += [_plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=ipu, grid_blocks=g) for ipu, g in ((16, 1), (64, 3))]
     return plans
 
 

@@ -184,3 +184,16 @@ def test_default_plans():
     assert g.as_flat().algo == nat.ALGO_FLAT
     capped = _plan.default_spmv_plan(skew, torch.float32, row_cap=32)
     assert capped.algo == nat.ALGO_ROWS and capped.row_cap == 32
+
+
+def test_batch_stacking_is_block_diagonal():
+    from flagsparse_public_b200 import batched, synthetic
+    mats = [synthetic.poisson_uniform(r, c, mean=m, seed=s, device="cpu")
+            for r, c, m, s in ((7, 5, 2.0, 1), (1, 9, 4.0, 2), (12, 12, 3.0, 3), (4, 3, 1.0, 4))]
+    mats.append((torch.zeros(0), torch.zeros(0, dtype=torch.int32), torch.zeros(3, dtype=torch.int64), (2, 6)))
+    data, indices, indptr, row_off, col_off = batched.stack_csr(mats)
+    assert row_off == [0, 7, 8, 20, 24, 26] and col_off == [0, 5, 14, 26, 29, 35]
+    assert indices.dtype == torch.int32 and indptr.dtype == torch.int64
+    got = torch.sparse_csr_tensor(indptr, indices.long(), data, size=(26, 35)).to_dense()
+    want = torch.block_diag(*[torch.sparse_csr_tensor(m[2], m[1].long(), m[0], size=m[3]).to_dense() for m in mats])
+    assert torch.equal(got, want)
