@@ -17,8 +17,10 @@ unit sizes and two column tiles.
   row-length mean / spread / maximum, distance from the diagonal, empty rows,
   dense width N), computed on the device (``fsb_csr_features``), and picks
   the lowest prediction.  It falls back to the autotuner when the features
-  lie outside the training range or its two best predictions are too close
-  to call.
+  lie outside the training range (a standardised feature beyond z_limit).
+  Near ties are not a reason to fall back: two plans predicted equal cost
+  about the same whichever is run (a positive ``margin`` makes the selector
+  fall back when its two best predictions differ by less than it).
 * ``train_mlp`` trains the network on the GPU with the project's own kernels
   (``fsb_mlp_forward`` / ``fsb_mlp_backward`` / ``fsb_adam_step``), full
   batch, deterministic.
@@ -271,7 +273,7 @@ class LearnedSelector:
     """Selector network with its feature standardisation; falls back to the
     autotuner outside the training range or on a near tie."""
 
-    def __init__(self, path=WEIGHTS_PATH, device="cuda", margin=0.05, z_limit=4.0, autotuner=None):
+    def __init__(self, path=WEIGHTS_PATH, device="cuda", margin=0.0, z_limit=4.0, autotuner=None):
         z = np.load(path, allow_pickle=False)
         names = tuple(str(s) for s in z["names"])
         if names != CANDIDATE_NAMES:

@@ -182,6 +182,10 @@ def test_default_plans():
     assert _plan.default_spmm_plan(banded, 32, torch.bfloat16).items_per_unit == 1024
     g = _plan.KernelPlan(nat.ALGO_GATHER, items_per_unit=256, fallback_ok=True)
     assert g.as_flat().algo == nat.ALGO_FLAT
+    long_skew = _plan.MatrixStats(1 << 20, 1 << 20, 156_953_476, 8192, 149.7, 780.0, 0)
+    p = _plan.default_spmv_plan(long_skew, torch.bfloat16)
+    assert p.algo == nat.ALGO_ROWS and p.lanes == 16
+    assert _plan.default_spmv_plan(long_skew, torch.float32).lanes == 32
     capped = _plan.default_spmv_plan(skew, torch.float32, row_cap=32)
     assert capped.algo == nat.ALGO_ROWS and capped.row_cap == 32
 
