@@ -189,6 +189,22 @@ int fsb_spmm_coo_atomic(const void* values, const void* row, const void* col,
                         const void* B, int64_t ldb, int64_t n_dense, void* C,
                         int64_t ldc, int acc_dtype, void* stream);
 
+/* ---- block-sparse SpMM on the tensor cores ----------------------------- *
+ * C (float32, n_rows x n_dense, row stride ldc) = A B for A in BSR form with
+ * dense 16 x 16 blocks: block_values[n_blocks][16][16] (row-major blocks,
+ * bf16 or f16: value_dtype = FSB_BF16 / FSB_F16), block_col[n_blocks] (block
+ * columns), block_row_ptr[ceil(n_rows / 16) + 1]; B (n_cols x n_dense, row
+ * stride ldb) has the same 16-bit type, is 16-byte aligned, with ldb and
+ * n_dense multiples of 8.  tcgen05.mma (kind::f16, fp32 accumulation in
+ * tensor memory), one MMA of 128 x 16 x 16 per stored block and 128-column
+ * tile.  No FlagSparse counterpart: FlagSparse runs block-structured
+ * matrices through its CSR SpMM (spmm_csr.py:2088-2157).                   */
+int fsb_bsr_spmm_tc(const void* block_values, int value_dtype,
+                    const void* block_col, int index_dtype,
+                    const void* block_row_ptr, int ptr_dtype, int64_t n_rows,
+                    int64_t n_cols, const void* B, int64_t ldb, int64_t n_dense,
+                    float* C, int64_t ldc, void* stream);
+
 /* ---- learned plan selector -------------------------------------------- *
  * No FlagSparse counterpart: FlagSparse picks its launch parameters by
  * fixed row-length buckets and device-property heuristics

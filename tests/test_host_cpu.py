@@ -201,3 +201,20 @@ def test_batch_stacking_is_block_diagonal():
     got = torch.sparse_csr_tensor(indptr, indices.long(), data, size=(26, 35)).to_dense()
     want = torch.block_diag(*[torch.sparse_csr_tensor(m[2], m[1].long(), m[0], size=m[3]).to_dense() for m in mats])
     assert torch.equal(got, want)
+
+
+def test_csr_to_bsr16_blocks_match_dense():
+    from flagsparse_public_b200 import bsr, synthetic
+    data, indices, indptr, shape = synthetic.poisson_uniform(37, 50, mean=6.0, seed=5, device="cpu")
+    vals, bcol, bptr = bsr.csr_to_bsr16(data, indices, indptr, shape, dtype=torch.float64)
+    dense = torch.sparse_csr_tensor(indptr, indices.long(), data.double(), size=shape).to_dense()
+    rebuilt = torch.zeros(48, 64, dtype=torch.float64)
+    for br in range(bptr.numel() - 1):
+        for b in range(int(bptr[br]), int(bptr[br + 1])):
+            c = int(bcol[b])
+            rebuilt[16 * br:16 * br + 16, 16 * c:16 * c + 16] = vals[b]
+    assert torch.equal(rebuilt[:37, :50], dense) and rebuilt[37:].abs().sum() == 0
+    assert bptr[0] == 0 and bptr[-1] == vals.shape[0] and bptr.numel() == 4
+    for br in range(3):  # block columns sorted within each block row
+        seg = bcol[int(bptr[br]):int(bptr[br + 1])]
+        assert torch.all(seg[1:] > seg[:-1])
