@@ -699,8 +699,125 @@ class BatchedUneven:
         return run, nbytes, f"every 16th matrix ({len(picks)} of {self.n_mats}), N = {self.n_dense}"
 
 
+class BsrTensorCore:
+    """Block-sparse matrix of dense 16 x 16 blocks (65536 block rows = 1,048,576
+    rows, 4 blocks per block row: the diagonal block and 3 uniform others;
+    64 nonzeros per row), bf16 values, B 1,048,576 x 128 bf16, C fp32.
+    Chosen form: BSR on the tensor cores (tcgen05, one 128 x 16 x 16 MMA per
+    block).  Plain form: the same matrix as CSR through the CUDA-core SpMM
+    (default plan, fp32 accumulation)."""
+
+    metric = "BSR 16x16 SpMM useful throughput (tensor cores)"
+    unit = "GB/s"
+    n_block_rows = 65536
+    blocks_per_row = 4
+    n_dense = 128
+
+    def generate(self, device):
+        from flagsparse_public_b200 import bsr, synthetic
+
+        data, indices, indptr, shape = synthetic.block_sparse(self.n_block_rows, self.blocks_per_row, seed=0,
+                                                              dtype=torch.bfloat16, device=device)
+        self.csr = (data, indices, indptr)
+        self.shape = shape
+        self.bsr = bsr.csr_to_bsr16(data, indices, indptr, shape)
+        self.B = synthetic.dense_operand(shape[1], self.n_dense, seed=1, dtype=torch.bfloat16, device=device)
+        self.n_blocks = int(self.bsr[0].shape[0])
+        self.nnz = int(data.numel())
+        self.useful_bytes = (self.n_blocks * (256 * 2 + 4) + shape[1] * self.n_dense * 2
+                             + shape[0] * self.n_dense * 4)
+        self.plain_bytes = self.nnz * 6 + shape[1] * self.n_dense * 2 + shape[0] * self.n_dense * 4
+        self.flops = 2 * self.n_blocks * 256 * self.n_dense
+
+    def build(self, device):
+        from flagsparse_public_b200 import _native as nat
+        from flagsparse_public_b200 import _plan, bsr
+
+        self.generate(device)
+        self.prepared = bsr.prepare_spmm_bsr(*self.bsr, self.shape)
+        self.C = torch.empty((self.shape[0], self.n_dense), dtype=torch.float32, device=device)
+        self.C_plain = torch.empty_like(self.C)
+        st = _plan.matrix_stats(self.csr[2], self.shape[0], self.shape[1])
+        self.plain_plan = _plan.default_spmm_plan(st, self.n_dense, torch.bfloat16)
+        self.acc = nat.ACC_NATIVE
+
+    def config(self):
+        return {"workload": "bsr16_blocksparse_65536x4blocks_1048576rows_n128_bf16",
+                "n_rows": self.shape[0], "n_blocks": self.n_blocks, "nnz": self.nnz, "n_dense": self.n_dense,
+                "global_batch": 1, "parallelism": "replicas",
+                "l2": "inputs larger than L2 (134 MB blocks + 268 MB B, 537 MB C); flushed before every timed step "
+                      "(256 MiB write)",
+                "tensor_flops_per_step": self.flops}
+
+    def step(self):
+        from flagsparse_public_b200 import bsr
+
+        bsr.flagsparse_spmm_bsr(B=self.B, prepared=self.prepared, out=self.C)
+
+    plain_desc = "same matrix as CSR, CUDA-core SpMM (fp32 accumulation), useful bytes of the CSR form"
+
+    def plain_step(self):
+        from flagsparse_public_b200 import _plan
+
+        d, i, p = self.csr
+        _plan.run_spmm(d, i, p, self.shape[0], self.shape[1], self.B, self.C_plain, self.acc, self.plain_plan)
+
+    def speedups(self, extra, ms_step, plain_ms):
+        return {}
+
+    def plan_desc(self):
+        return {"kind": "bsr16_tcgen05", "tile_columns": 128, "mma": "128x16x16 kind::f16, fp32 in TMEM"}
+
+    def force_plan(self, plan):
+        self.plain_plan = plan
+
+    def host_inputs(self):
+        vals, bcol, bptr = self.bsr
+        self.h = [t.cpu().pin_memory() for t in (vals, bcol, bptr, self.B)]
+        self.h_out = torch.empty(self.C.shape, dtype=torch.float32).pin_memory()
+        self.h2d_bytes = sum(t.numel() * t.element_size() for t in self.h)
+        self.d2h_bytes = self.h_out.numel() * 4
+
+    def e2e_step(self, device):
+        from flagsparse_public_b200 import bsr
+
+        d = [t.to(device, non_blocking=True) for t in self.h]
+        C = bsr.flagsparse_spmm_bsr(d[0], d[1], d[2], d[3], self.shape)
+        self.h_out.copy_(C, non_blocking=True)
+
+    def fp64_error(self):
+        from oracle import oracle as orc
+        from tests.numerics import scaled_error
+
+        self.step()
+        self.plain_step()
+        torch.cuda.synchronize()
+        rows = 4096
+        d, i, p = (t.cpu() for t in self.csr)
+        end = int(p[rows])
+        sub = (d[:end], i[:end], p[:rows + 1])
+        exact, mag = orc.spmm_csr_exact(*sub, self.B.cpu())
+        return {"chosen": scaled_error(self.C[:rows], exact, mag), "plain": scaled_error(self.C_plain[:rows], exact, mag),
+                "definition": "max |c - c64| / sum_k |a_k b_k| over the first 4096 rows (FP64 of the same bf16 inputs)"}
+
+    def cpu_step_factory(self, threads, sample_rows=None):
+        from oracle import oracle as orc
+
+        rows = 16384
+        d, i, p = (t.cpu() for t in self.csr)
+        end = int(p[rows])
+        sub = (d[:end], i[:end], p[:rows + 1])
+        Bh = self.B.cpu()
+        nbytes = end * 6 + rows * self.n_dense * 6
+
+        def run():
+            orc.spmm_csr(*sub, Bh, acc_mode=orc.ACC_NATIVE, out_dtype=torch.float32, threads=threads)
+
+        return run, nbytes, f"rows [0, {rows}) as CSR (bf16 inputs, fp32 accumulation), N = {self.n_dense}"
+
+
 WORKLOADS = {"spmm_powerlaw": SpmmPowerlaw, "spmv_poisson": SpmvPoisson, "precision_banded": PrecisionBanded,
-             "batched_uneven": BatchedUneven}
+             "batched_uneven": BatchedUneven, "bsr_tensor_core": BsrTensorCore}
 
 
 # ------------------------------------------------------------------ timing --

@@ -15,6 +15,7 @@ hold any nonzero are stored dense, zero-filled), so a CSR user can switch.
 import torch
 
 from . import _native as nat
+from . import _plan
 
 BLOCK = 16
 BSR_VALUE_DTYPES = (torch.bfloat16, torch.float16)
@@ -106,4 +107,5 @@ def flagsparse_spmm_bsr(block_values=None, block_col=None, block_row_ptr=None, B
                              nat.dtype_code(p.block_row_ptr.dtype), p.shape[0], p.shape[1], nat.ptr(B),
                              int(B.stride(0)), n_dense, nat.ptr(C), int(C.stride(0)), nat.stream_handle(B.device))
     nat.check(rc, "fsb_bsr_spmm_tc")
+    _plan.LAUNCHES["count"] += 1 if p.shape[0] and n_dense else 0
     return C

@@ -54,12 +54,30 @@ k_spmm_merge_fixup(const int64_t* __restrict__ carry_row, const A* __restrict__ 
     const int64_t r = carry_row[t];
     if (r < 0) return;
     if (t > 0 && carry_row[t - 1] == r) return;
+    // end of the run of units carrying row r: 32 entries per step, first
+    // mismatch by ballot (a long row spans many units)
     int64_t u_end = t + 1;
-    while (u_end < n_units && carry_row[u_end] == r) ++u_end;
+    while (true) {
+        const int64_t u = u_end + lane;
+        const bool same = u < n_units && carry_row[u] == r;
+        const unsigned stop = __ballot_sync(0xffffffffu, !same);
+        if (stop) {
+            u_end += __ffs(stop) - 1;
+            break;
+        }
+        u_end += 32;
+    }
     const int64_t out_row = row_map ? idx(row_map[idx(ptr[r])]) : r;
     for (int64_t c = lane; c < n_dense; c += 32) {
+        // loads four carries ahead, adds in unit order (deterministic)
         A sum = carry_val[t * n_dense + c];
-        for (int64_t u = t + 1; u < u_end; ++u) sum = acc_add(sum, carry_val[u * n_dense + c]);
+        int64_t u = t + 1;
+        for (; u + 4 <= u_end; u += 4) {
+            const A a0 = carry_val[u * n_dense + c], a1 = carry_val[(u + 1) * n_dense + c];
+            const A a2 = carry_val[(u + 2) * n_dense + c], a3 = carry_val[(u + 3) * n_dense + c];
+            sum = acc_add(acc_add(acc_add(acc_add(sum, a0), a1), a2), a3);
+        }
+        for (; u < u_end; ++u) sum = acc_add(sum, carry_val[u * n_dense + c]);
         if (u_end < n_units) sum = acc_add(sum, head_val[u_end * n_dense + c]);
         C[out_row * ldc + c] = Out<O, A>::cvt(sum);
     }
