@@ -80,9 +80,14 @@ def prepare_spmm_bsr(block_values, block_col, block_row_ptr, shape):
 
 
 def flagsparse_spmm_bsr(block_values=None, block_col=None, block_row_ptr=None, B=None, shape=None, prepared=None,
-                        out=None):
+                        out=None, staging="auto"):
     """C = A B (fp32) for a BSR matrix of dense 16 x 16 blocks on the tensor
-    cores; B row-major with the values' 16-bit type, columns a multiple of 8."""
+    cores; B row-major with the values' 16-bit type, columns a multiple of 8.
+    ``staging``: "tma" (B slices loaded by the Tensor Memory Accelerator),
+    "threads" (loaded by the CTA's threads) or "auto" (TMA where a tensor map
+    can be encoded for B, else threads)."""
+    if staging not in ("auto", "tma", "threads"):
+        raise ValueError('staging must be "auto", "tma" or "threads"')
     if prepared is None:
         prepared = PreparedBsr(block_values, block_col, block_row_ptr, shape)
     p = prepared
@@ -102,10 +107,17 @@ def flagsparse_spmm_bsr(block_values=None, block_col=None, block_row_ptr=None, B
     if out is not None and (out.dtype != torch.float32 or out.shape != (p.shape[0], n_dense) or not out.is_contiguous()):
         raise ValueError("out must be a contiguous float32 tensor of shape (n_rows, n_dense)")
     lib = nat.library()
-    rc = lib.fsb_bsr_spmm_tc(nat.ptr(p.block_values), nat.dtype_code(p.block_values.dtype), nat.ptr(p.block_col),
-                             nat.dtype_code(p.block_col.dtype), nat.ptr(p.block_row_ptr),
-                             nat.dtype_code(p.block_row_ptr.dtype), p.shape[0], p.shape[1], nat.ptr(B),
-                             int(B.stride(0)), n_dense, nat.ptr(C), int(C.stride(0)), nat.stream_handle(B.device))
+
+    def launch(mode):
+        return lib.fsb_bsr_spmm_tc(nat.ptr(p.block_values), nat.dtype_code(p.block_values.dtype),
+                                   nat.ptr(p.block_col), nat.dtype_code(p.block_col.dtype), nat.ptr(p.block_row_ptr),
+                                   nat.dtype_code(p.block_row_ptr.dtype), p.shape[0], p.shape[1], nat.ptr(B),
+                                   int(B.stride(0)), n_dense, nat.ptr(C), int(C.stride(0)), mode,
+                                   nat.stream_handle(B.device))
+
+    rc = launch(nat.BSR_STAGE_THREADS if staging == "threads" else nat.BSR_STAGE_TMA)
+    if rc == nat.FSB_ERR_UNSUPPORTED and staging == "auto":
+        rc = launch(nat.BSR_STAGE_THREADS)
     nat.check(rc, "fsb_bsr_spmm_tc")
     _plan.LAUNCHES["count"] += 1 if p.shape[0] and n_dense else 0
     return C

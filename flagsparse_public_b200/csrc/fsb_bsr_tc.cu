@@ -19,11 +19,23 @@
 // block after next.  At the end each warp reads its 32 TMEM lanes
 // (tcgen05.ld 32x32b.x16) and stores 16 rows of C, coalesced along columns.
 //
+// Two stagings of the B slices:
+//   * k_bsr_spmm_tma (default): the Tensor Memory Accelerator loads each
+//     slice as two 64-column x 16-row boxes of a 2-D tensor map over B
+//     (128-byte swizzle) into a 4-stage ring, one thread keeping three blocks
+//     in flight ahead of the MMAs (SWIZZLE_128B MN-major operand);
+//   * k_bsr_spmm_tc: the CTA's threads copy the slice with 16-byte loads into
+//     two alternating stages (SWIZZLE_NONE MN-major operand).
+//
 // TMEM: 32 columns per CTA; at most 16 CTAs of 128 threads are resident per
 // SM, so allocations never exceed the SM's 512 columns and never wait.
 // Every mbarrier wait is bounded (1 s, globaltimer); on expiry the kernel
 // records FSB_ERR_TIMEOUT in the device error word (fsb_device_error), waits
 // (bounded) for the MMA it issued, frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
+#include <mutex>
 #include <type_traits>
 
 #include "fsb_dispatch.cuh"
@@ -230,12 +242,214 @@ k_bsr_spmm_tc(const V* __restrict__ blocks, const I* __restrict__ bcol, const P*
     }
 }
 
+constexpr int kTmaStages = 4;
+constexpr int kTmaBoxCols = 64;                      // 128 bytes of 16-bit values
+constexpr int kTmaBoxBytes = kTmaBoxCols * 16 * 2;  // 2 KB per box, 2 boxes per slice
+
+// Descriptor of a SWIZZLE_128B MN-major operand (layout type 2): 64-column x
+// 8-row atoms of 1 KB; LBO = byte stride between 64-column groups, SBO =
+// byte stride between 8-row K groups.
+__device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    return smem_desc(addr, lbo, sbo) | (2ull << 61);
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
+            "r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        : "memory");
+}
+
+template <class V, class I, class P>
+__global__ void __launch_bounds__(kThreads)
+k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const V* __restrict__ blocks, const I* __restrict__ bcol,
+               const P* __restrict__ bptr, int64_t n_rows, int64_t n_dense, float* __restrict__ C, int64_t ldc,
+               int* __restrict__ err) {
+    constexpr bool kBf16 = std::is_same<V, __nv_bfloat16>::value;
+    constexpr int S = kTmaStages;
+    constexpr uint32_t kSliceBytes = 2 * kTmaBoxBytes;
+    __shared__ __align__(1024) unsigned char sa[S][2 * kTmaBoxBytes];
+    __shared__ __align__(128) unsigned char sb[S][kBStageBytes];
+    __shared__ __align__(8) uint64_t full[S], empty[S];
+    __shared__ uint32_t tmem_base_slot;
+    __shared__ int fail_flag;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int64_t r = blockIdx.x;
+    const int64_t c0 = (int64_t)blockIdx.y * kM;
+    const int cols = (int)((n_dense - c0) < kM ? (n_dense - c0) : kM);
+    const int64_t b0 = idx(bptr[r]), b1 = idx(bptr[r + 1]);
+    const int nb = (int)(b1 - b0);
+
+    auto issue = [&](int b) {  // thread 0: slice of block b into stage b % S
+        const int s = b % S;
+        const uint32_t bar = smem_u32(&full[s]);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kSliceBytes)
+                     : "memory");
+        const int y = (int)(idx(bcol[b0 + b]) * 16);
+        tma_load_2d(smem_u32(&sa[s][0]), &bmap, (int)c0, y, bar);
+        tma_load_2d(smem_u32(&sa[s][kTmaBoxBytes]), &bmap, (int)c0 + kTmaBoxCols, y, bar);
+    };
+
+    if (tid == 0) {
+        for (int i = 0; i < S; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[i])) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[i])) : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        fail_flag = 0;
+    }
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base_slot)),
+                     "r"(kTmemCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_slot;
+    constexpr uint32_t idesc = instr_desc<kBf16>();
+    if (tid == 0)
+        for (int b = 0; b < nb && b < S; ++b) issue(b);
+
+    int issued = nb < S ? nb : S;  // meaningful in thread 0 only
+    bool failed = false;
+    for (int b = 0; b < nb; ++b) {
+        const int s = b % S;
+        // the block's 16 x 16 values, K-major: (n, k) at (n % 8) * 16 +
+        // (k % 8) * 2 + (n / 8) * 256 + (k / 8) * 128.  Stage s was freed
+        // by thread 0's wait on empty[s] before it refilled the stage, which
+        // precedes this iteration's barrier.
+        if (tid < 32) {
+            const int n = tid >> 1, kc = tid & 1;
+            const uint4 v = ld_vec16(blocks + (b0 + b) * 256 + n * 16 + kc * 8);
+            *reinterpret_cast<uint4*>(&sb[s][(n & 7) * 16 + (n >> 3) * 256 + kc * 128]) = v;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        if (__syncthreads_or(fail_flag)) {
+            failed = true;
+            break;
+        }
+        if (tid == 0) {
+            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((b / S) & 1))) {
+                fail_flag = 1;
+            } else {
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                // A: two 64-column groups 2 KB apart (LBO), 8-row groups 1 KB apart (SBO)
+                const uint64_t adesc = smem_desc_sw128(smem_u32(&sa[s][0]), kTmaBoxBytes, 1024);
+                const uint64_t bdesc = smem_desc(smem_u32(&sb[s][0]), 128, 256);
+                const uint32_t accumulate = b > 0 ? 1u : 0u;
+                const uint32_t zero = 0;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                    "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(zero), "r"(zero), "r"(zero),
+                    "r"(zero)
+                    : "memory");
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&empty[s]))
+                             : "memory");
+                if (b + S < nb) {
+                    // refill stage s with block b + S once this MMA has read it
+                    if (!mbar_wait(smem_u32(&empty[s]), (uint32_t)((b / S) & 1))) {
+                        fail_flag = 1;
+                    } else {
+                        issue(b + S);
+                        ++issued;
+                    }
+                }
+            }
+        }
+    }
+    if (nb > 0 && !failed) {
+        const int last = nb - 1;
+        const bool ok = mbar_wait(smem_u32(&empty[last % S]), (uint32_t)((last / S) & 1));
+        failed = __syncthreads_or(!ok || fail_flag) != 0;
+    }
+    if (failed) {
+        if (tid == 0) {
+            atomicExch(err, FSB_ERR_TIMEOUT);
+            // drain (bounded) the copies and MMAs this CTA started
+            for (int b = 0; b < issued; ++b) mbar_wait(smem_u32(&full[b % S]), (uint32_t)((b / S) & 1));
+            for (int b = issued > S ? issued - S : 0; b < issued; ++b)
+                mbar_wait(smem_u32(&empty[b % S]), (uint32_t)((b / S) & 1));
+        }
+    } else {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        uint32_t d[16];
+        if (nb > 0) {
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15}, [%16];"
+                : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
+                  "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]),
+                  "=r"(d[15])
+                : "r"(taddr)
+                : "memory");
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+        } else {
+#pragma unroll
+            for (int n = 0; n < 16; ++n) d[n] = 0u;
+        }
+        const int m = warp * 32 + lane;
+        if (m < cols) {
+#pragma unroll
+            for (int n = 0; n < 16; ++n) {
+                const int64_t row = r * 16 + n;
+                if (row < n_rows) __stcs(C + row * ldc + c0 + m, __uint_as_float(d[n]));
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols) : "memory");
+    }
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (once).
+static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
+    static std::once_flag once;
+    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+    });
+    return fn;
+}
+
+// 2-D tensor map over B (columns innermost): 64 x 16 boxes, 128-byte swizzle,
+// zero fill outside the matrix.  False when it cannot be encoded.
+static bool encode_b_map(CUtensorMap* map, int value_dtype, const void* B, int64_t n_cols, int64_t ldb,
+                         int64_t n_dense) {
+    auto fn = encode_fn();
+    if (!fn) return false;
+    const cuuint64_t dims[2] = {(cuuint64_t)n_dense, (cuuint64_t)n_cols};
+    const cuuint64_t strides[1] = {(cuuint64_t)ldb * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)kTmaBoxCols, 16};
+    const cuuint32_t estr[2] = {1, 1};
+    const CUresult rc = fn(map, value_dtype == FSB_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                           2, const_cast<void*>(B), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return rc == CUDA_SUCCESS;
+}
+
 }  // namespace bsr
 }  // namespace fsb
 
 extern "C" int fsb_bsr_spmm_tc(const void* block_values, int value_dtype, const void* block_col, int index_dtype,
                                const void* block_row_ptr, int ptr_dtype, int64_t n_rows, int64_t n_cols,
-                               const void* B, int64_t ldb, int64_t n_dense, float* C, int64_t ldc, void* stream) {
+                               const void* B, int64_t ldb, int64_t n_dense, float* C, int64_t ldc, int staging,
+                               void* stream) {
     if (value_dtype != FSB_BF16 && value_dtype != FSB_F16) {
         fsb_host::set_error("fsb_bsr_spmm_tc: values and B must be bfloat16 or float16");
         return FSB_ERR_UNSUPPORTED;
@@ -265,8 +479,35 @@ extern "C" int fsb_bsr_spmm_tc(const void* block_values, int value_dtype, const 
         fsb_host::set_error("fsb_bsr_spmm_tc: cannot resolve the device error word");
         return FSB_ERR_LAUNCH;
     }
+    if (staging != FSB_BSR_STAGE_TMA && staging != FSB_BSR_STAGE_THREADS) {
+        fsb_host::set_error("fsb_bsr_spmm_tc: staging must be FSB_BSR_STAGE_TMA or FSB_BSR_STAGE_THREADS");
+        return FSB_ERR_INVALID;
+    }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     dim3 g((unsigned)n_block_rows, (unsigned)tiles);
+    CUtensorMap bmap;
+    if (staging == FSB_BSR_STAGE_TMA) {
+        if (n_cols >= 0x7fffffffLL || n_dense >= 0x7fffffffLL ||
+            !fsb::bsr::encode_b_map(&bmap, value_dtype, B, n_cols, ldb, n_dense)) {
+            fsb_host::set_error("fsb_bsr_spmm_tc: no tensor map can be encoded for B (use FSB_BSR_STAGE_THREADS)");
+            return FSB_ERR_UNSUPPORTED;
+        }
+        return fsb::dispatch_idx(index_dtype, [&](auto ti) -> int {
+            using I = typename decltype(ti)::type;
+            return fsb::dispatch_idx(ptr_dtype, [&](auto tp) -> int {
+                using P = typename decltype(tp)::type;
+                if (value_dtype == FSB_BF16)
+                    fsb::bsr::k_bsr_spmm_tma<__nv_bfloat16, I, P><<<g, fsb::bsr::kThreads, 0, st>>>(
+                        bmap, static_cast<const __nv_bfloat16*>(block_values), static_cast<const I*>(block_col),
+                        static_cast<const P*>(block_row_ptr), n_rows, n_dense, C, ldc, err);
+                else
+                    fsb::bsr::k_bsr_spmm_tma<__half, I, P><<<g, fsb::bsr::kThreads, 0, st>>>(
+                        bmap, static_cast<const __half*>(block_values), static_cast<const I*>(block_col),
+                        static_cast<const P*>(block_row_ptr), n_rows, n_dense, C, ldc, err);
+                return fsb_host::check_launch("k_bsr_spmm_tma");
+            });
+        });
+    }
     return fsb::dispatch_idx(index_dtype, [&](auto ti) -> int {
         using I = typename decltype(ti)::type;
         return fsb::dispatch_idx(ptr_dtype, [&](auto tp) -> int {

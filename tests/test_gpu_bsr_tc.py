@@ -28,28 +28,34 @@ def _check(vals, bcol, bptr, shape, B, C):
     assert err <= 1e-5, err
 
 
+STAGINGS = ["tma", "threads"]
+
+
+@pytest.mark.parametrize("staging", STAGINGS)
 @pytest.mark.parametrize("n_dense", [8, 32, 128])
-def test_block_diagonal_single_tile(n_dense):
+def test_block_diagonal_single_tile(n_dense, staging):
     data, indices, indptr, shape = synthetic.block_sparse(8, 1, seed=1, dtype=torch.bfloat16, device=DEV)
     vals, bcol, bptr = bsr.csr_to_bsr16(data, indices, indptr, shape)
     B = synthetic.dense_operand(shape[1], n_dense, seed=2, dtype=torch.bfloat16, device=DEV)
-    C = bsr.flagsparse_spmm_bsr(vals, bcol, bptr, B, shape)
+    C = bsr.flagsparse_spmm_bsr(vals, bcol, bptr, B, shape, staging=staging)
     torch.cuda.synchronize()
     _check(vals, bcol, bptr, shape, B, C)
 
 
+@pytest.mark.parametrize("staging", STAGINGS)
 @pytest.mark.parametrize("dtype", [torch.bfloat16, torch.float16])
 @pytest.mark.parametrize("n_dense", [16, 136, 256])
-def test_block_sparse_many_blocks_per_row(dtype, n_dense):
-    data, indices, indptr, shape = synthetic.block_sparse(300, 5, seed=3, dtype=dtype, device=DEV)
+def test_block_sparse_many_blocks_per_row(dtype, n_dense, staging):
+    data, indices, indptr, shape = synthetic.block_sparse(300, 9, seed=3, dtype=dtype, device=DEV)
     vals, bcol, bptr = bsr.csr_to_bsr16(data, indices, indptr, shape)
     B = synthetic.dense_operand(shape[1], n_dense, seed=4, dtype=dtype, device=DEV)
-    C = bsr.flagsparse_spmm_bsr(vals, bcol, bptr, B, shape)
+    C = bsr.flagsparse_spmm_bsr(vals, bcol, bptr, B, shape, staging=staging)
     torch.cuda.synchronize()
     _check(vals, bcol, bptr, shape, B, C)
 
 
-def test_ragged_shapes_empty_block_rows_and_repeat_calls():
+@pytest.mark.parametrize("staging", STAGINGS)
+def test_ragged_shapes_empty_block_rows_and_repeat_calls(staging):
     # 37 x 45: partial last block row and block column; rows 16..31 empty
     data, indices, indptr, shape = synthetic.poisson_uniform(37, 45, mean=9.0, seed=6, dtype=torch.bfloat16,
                                                              device=DEV)
@@ -65,7 +71,18 @@ def test_ragged_shapes_empty_block_rows_and_repeat_calls():
     B = synthetic.dense_operand(45, 24, seed=7, dtype=torch.bfloat16, device=DEV)
     for _ in range(2):
         C = torch.full((37, 24), float("nan"), device=DEV)
-        bsr.flagsparse_spmm_bsr(vals, bcol, bptr, B, shape, out=C)
+        bsr.flagsparse_spmm_bsr(vals, bcol, bptr, B, shape, out=C, staging=staging)
         torch.cuda.synchronize()
         _check(vals, bcol, bptr, shape, B, C)
         assert torch.all(C[16:32] == 0)
+
+
+def test_staging_paths_agree_bitwise():
+    """Both stagings feed the same MMAs in the same order."""
+    data, indices, indptr, shape = synthetic.block_sparse(500, 6, seed=8, dtype=torch.bfloat16, device=DEV)
+    vals, bcol, bptr = bsr.csr_to_bsr16(data, indices, indptr, shape)
+    B = synthetic.dense_operand(shape[1], 128, seed=9, dtype=torch.bfloat16, device=DEV)
+    a = bsr.flagsparse_spmm_bsr(vals, bcol, bptr, B, shape, staging="tma")
+    b = bsr.flagsparse_spmm_bsr(vals, bcol, bptr, B, shape, staging="threads")
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
