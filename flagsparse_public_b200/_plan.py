@@ -140,9 +140,10 @@ def _vec_elems(dtype):
 
 def default_spmv_plan(stats, dtype, row_cap=0):
     """Heuristic SpMV plan: merge path for skewed rows that are short on
-    average, else row groups sized so a row's nonzeros take about one 16-byte
-    vector per lane (long average rows keep 16-32 lanes busy even when a few
-    rows are much longer: measured faster than merge path there)."""
+    average, else row groups sized so a row's nonzeros take about half a
+    16-byte vector per lane (more lanes shorten each row's dependent load
+    chain; long average rows keep 16-32 lanes busy even when a few rows are
+    much longer: measured faster than merge path there)."""
     if row_cap > 0 or stats.n_rows == 0:
         lanes = _pow2_clamp(stats.mean_row / _vec_elems(dtype), 2, 32) if stats.n_rows else 32
         return KernelPlan(nat.ALGO_ROWS, lanes=lanes, row_cap=row_cap)
@@ -150,7 +151,7 @@ def default_spmv_plan(stats, dtype, row_cap=0):
     if skewed and stats.mean_row < 32:
         ipt = 8 if torch.empty((), dtype=dtype).element_size() <= 4 else 4
         return KernelPlan(nat.ALGO_MERGE, items_per_unit=SPMV_MERGE_THREADS * ipt)
-    lanes = _pow2_clamp(stats.mean_row / _vec_elems(dtype), 2, 32)
+    lanes = _pow2_clamp(2 * stats.mean_row / _vec_elems(dtype), 2, 32)
     return KernelPlan(nat.ALGO_ROWS, lanes=lanes)
 
 

@@ -172,7 +172,7 @@ def test_coo_fallback_policy(monkeypatch):
 def test_default_plans():
     flat = _plan.MatrixStats(16384, 16384, 262144, 35, 16.0, 4.0, 0)
     p = _plan.default_spmv_plan(flat, torch.float32)
-    assert p.algo == nat.ALGO_ROWS and p.lanes == 4
+    assert p.algo == nat.ALGO_ROWS and p.lanes == 8
     skew = _plan.MatrixStats(262144, 262144, 3_100_000, 7200, 11.9, 80.0, 10)
     assert _plan.default_spmv_plan(skew, torch.float32).algo == nat.ALGO_MERGE
     mm = _plan.default_spmm_plan(skew, 64, torch.float32)
@@ -184,7 +184,7 @@ def test_default_plans():
     assert g.as_flat().algo == nat.ALGO_FLAT
     long_skew = _plan.MatrixStats(1 << 20, 1 << 20, 156_953_476, 8192, 149.7, 780.0, 0)
     p = _plan.default_spmv_plan(long_skew, torch.bfloat16)
-    assert p.algo == nat.ALGO_ROWS and p.lanes == 16
+    assert p.algo == nat.ALGO_ROWS and p.lanes == 32
     assert _plan.default_spmv_plan(long_skew, torch.float32).lanes == 32
     capped = _plan.default_spmv_plan(skew, torch.float32, row_cap=32)
     assert capped.algo == nat.ALGO_ROWS and capped.row_cap == 32
