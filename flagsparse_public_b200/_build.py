@@ -1,6 +1,7 @@
 """Build recipe for the sm_100a CUDA library behind the C ABI.
 
-``build()`` compiles every ``csrc/*.cu`` file with nvcc for sm_100a only
+``build()`` compiles every ``csrc/*.cu`` file with nvcc for sm_100a only (and
+the host-only ``csrc/*.cpp`` files with nvcc's host compiler, ``-pthread``)
 (``-gencode arch=compute_100a,code=sm_100a``) into
 ``flagsparse_public_b200/libflagsparse_b200.so``, in-tree, so the library
 travels with the source tree.  It needs nvcc but no GPU.
@@ -26,7 +27,7 @@ NVCC_FLAGS = [
     "-lineinfo",
     "--expt-relaxed-constexpr",
     "-Xcompiler",
-    "-fPIC,-O3",
+    "-fPIC,-O3,-pthread",
     "-DNDEBUG",
     "-I" + os.path.join(ROOT, "include"),
 ]
@@ -41,7 +42,7 @@ def _nvcc():
 
 def _sources():
     return sorted(
-        os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith(".cu")
+        os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cu", ".cpp"))
     )
 
 
@@ -59,7 +60,7 @@ def _stale(target, deps):
 
 
 def _compile(src, verbose):
-    obj = os.path.join(OBJ_DIR, os.path.basename(src).replace(".cu", ".o"))
+    obj = os.path.join(OBJ_DIR, os.path.splitext(os.path.basename(src))[0] + ".o")
     if not _stale(obj, [src] + _headers()):
         return obj
     cmd = [_nvcc()] + ARCH_FLAGS + NVCC_FLAGS + ["-c", src, "-o", obj]
@@ -82,7 +83,7 @@ def build(verbose=False, jobs=None):
     with concurrent.futures.ThreadPoolExecutor(max_workers=jobs) as ex:
         objs = list(ex.map(lambda s: _compile(s, verbose), srcs))
     if _stale(LIB_PATH, objs):
-        cmd = [_nvcc()] + ARCH_FLAGS + ["-shared", "-o", LIB_PATH] + objs
+        cmd = [_nvcc()] + ARCH_FLAGS + ["-shared", "-o", LIB_PATH] + objs + ["-lpthread"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

@@ -120,6 +120,13 @@ _SIGNATURES = {
          ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
          ctypes.c_int, ctypes.c_void_p],
     ),
+    "fsb_mtx_open": (
+        ctypes.c_void_p,
+        [ctypes.c_char_p, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_int64),
+         ctypes.POINTER(ctypes.c_int64), ctypes.c_int],
+    ),
+    "fsb_mtx_read": (ctypes.c_int, [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]),
+    "fsb_mtx_close": (None, [ctypes.c_void_p]),
     "fsb_csr_features": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int64,

@@ -210,6 +210,22 @@ int fsb_bsr_spmm_tc(const void* block_values, int value_dtype,
                     int64_t n_cols, const void* B, int64_t ldb, int64_t n_dense,
                     float* C, int64_t ldc, int staging, void* stream);
 
+/* ---- Matrix Market ingest (host) ------------------------------------- *
+ * Parses a .mtx coordinate file into CSR (float64 values, int64 indices and
+ * row offsets, columns sorted in each row) with the semantics of FlagSparse's
+ * loader load_mtx_to_csr_torch (tests/test_spmv.py:103-178): pattern
+ * entries 1.0, duplicates summed in file order, symmetric / hermitian
+ * entries mirrored, skew-symmetric ones mirrored negated, out-of-range
+ * entries dropped.  fsb_mtx_open parses (threads <= 0: all host threads) and
+ * returns a handle (null on error, message in fsb_last_error) with the sizes;
+ * fsb_mtx_read copies into caller arrays of n_rows + 1 / nnz / nnz entries;
+ * fsb_mtx_close frees the handle.  No GPU involved.                       */
+void* fsb_mtx_open(const char* path, int64_t* n_rows, int64_t* n_cols,
+                   int64_t* nnz, int threads);
+int   fsb_mtx_read(void* handle, int64_t* indptr, int64_t* indices,
+                   double* values);
+void  fsb_mtx_close(void* handle);
+
 /* ---- learned plan selector -------------------------------------------- *
  * No FlagSparse counterpart: FlagSparse picks its launch parameters by
  * fixed row-length buckets and device-property heuristics
