@@ -32,6 +32,9 @@ _EXPORTS = {
     "flagsparse_spmm_csr_opt": "spmm_csr",
     "flagsparse_spmm_csr_opt_alg2": "spmm_csr_opt_alg2",
     "flagsparse_spmm_coo": "spmm_coo",
+    "SDDMMPrepared": "sddmm_csr",
+    "prepare_sddmm_csr": "sddmm_csr",
+    "flagsparse_sddmm_csr": "sddmm_csr",
     "PreparedCsrMixed": "precision",
     "prepare_csr_mixed": "precision",
     "flagsparse_spmv_csr_mixed": "precision",

@@ -210,6 +210,19 @@ int fsb_bsr_spmm_tc(const void* block_values, int value_dtype,
                     int64_t n_cols, const void* B, int64_t ldb, int64_t n_dense,
                     float* C, int64_t ldc, int staging, void* stream);
 
+/* ---- SDDMM ------------------------------------------------------------- *
+ * out[p] = alpha * dot(x[row_ids[p]], y[col_idx[p]]) + beta * data[p] for
+ * the nnz stored positions of a CSR pattern (data may be null: beta term
+ * dropped); x (n_rows x k, row stride ldx) and y (n_cols x k, row stride
+ * ldy) row-major, float32 (float32 accumulation) or float64.  Replaces the
+ * launch of _sddmm_csr_real_kernel in _run_sddmm_prepared
+ * (sddmm_csr.py:271-348).                                                  */
+int fsb_sddmm_csr(const void* col_idx, int index_dtype, const int32_t* row_ids,
+                  int64_t nnz, int64_t n_rows, int64_t n_cols, const void* x,
+                  int64_t ldx, const void* y, int64_t ldy, int64_t k,
+                  const void* data, void* out, int value_dtype, double alpha,
+                  double beta, void* stream);
+
 /* ---- Matrix Market ingest (host) ------------------------------------- *
  * Parses a .mtx coordinate file into CSR (float64 values, int64 indices and
  * row offsets, columns sorted in each row) with the semantics of FlagSparse's
