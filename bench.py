@@ -64,13 +64,17 @@ def dist_env():
     return int(os.environ.get("RANK", 0)), int(os.environ.get("WORLD_SIZE", 1)), int(os.environ.get("LOCAL_RANK", 0))
 
 
-def init_dist(world):
+def init_dist(world, backend=None):
+    """One process per GPU: NCCL where CUDA is present, gloo otherwise (CPU
+    tests of the multi-rank path).  Short timeout: ranks that wait on a
+    missing peer end with an error instead of hanging."""
     if world > 1:
         import datetime
 
         import torch.distributed as dist
 
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+        backend = backend or ("nccl" if torch.cuda.is_available() else "gloo")
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
 
 
 def barrier(world):
@@ -85,9 +89,16 @@ def max_over_ranks(value, world):
         return value
     import torch.distributed as dist
 
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def aggregate_value(units_per_rank, world, max_ms):
+    """Whole-job throughput: the units every rank processed over the slowest
+    rank's time (weak scaling: each rank runs the full workload)."""
+    return units_per_rank * world / (max_ms * 1e-3) / 1e9
 
 
 def measured_peak_hbm():
@@ -616,7 +627,7 @@ class BatchedUneven:
                 "matrices": self.n_mats, "n_rows_total": self.rows, "nnz": self.nnz, "n_dense": self.n_dense,
                 "global_batch": self.n_mats, "parallelism": "replicas",
                 "l2": "inputs larger than L2 (4.3 GB); flushed before every timed step (256 MiB write)",
-                "autotune_ms": self.prep.timings}
+                "autotune_ms": self.prep.timings if hasattr(self, "prep") else None}
 
     def step(self):
         self.prep.graph.replay()
@@ -925,7 +936,7 @@ def run_ours(args):
     barrier(world)
     total_ms = max_over_ranks(sum(times), world)
     ms_step = total_ms / args.steps
-    value = wl.useful_bytes * world / (ms_step * 1e-3) / 1e9
+    value = aggregate_value(wl.useful_bytes, world, ms_step)
     if args.profile:
         if rank == 0:
             print(json.dumps({"profile_run": True, "ms_per_step": ms_step}), flush=True)
