@@ -12,6 +12,11 @@
 
 namespace fsb {
 
+// Merge-path units of the SpMM kernels hold at most this many items (rows +
+// nonzeros; a unit's nonzero count is kept in 32 bits).  Unit coordinates
+// must come from fsb_merge_partition for the same matrix and items.
+constexpr int32_t kMaxItemsPerUnit = 1 << 24;
+
 // ---------------------------------------------------------------- types ----
 struct __align__(8) c64_t { float re, im; };
 struct __align__(16) c128_t { double re, im; };

@@ -352,7 +352,7 @@ int launch_spmm_flat(const fsb_csr* Am, const V* val, const I* col, const P* ptr
                      int64_t ldb, int64_t n_dense, O* C, int64_t ldc, const fsb_plan* plan, void* workspace,
                      int64_t workspace_bytes, cudaStream_t st) {
     const int64_t n_units = plan->n_units;
-    if (plan->items_per_unit < 1 || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
+    if (plan->items_per_unit < 1 || plan->items_per_unit > kMaxItemsPerUnit || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
         !plan->unit_coords) {
         fsb_host::set_error("fsb_spmm_csr: flat plan does not match the matrix");
         return FSB_ERR_INVALID;
@@ -445,7 +445,7 @@ int launch_spmm(const fsb_csr* Am, const V* val, const I* col, const P* ptr, con
         return FSB_ERR_INVALID;
     }
     const int64_t n_units = plan->n_units;
-    if (plan->items_per_unit < 1 || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
+    if (plan->items_per_unit < 1 || plan->items_per_unit > kMaxItemsPerUnit || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
         !plan->unit_coords) {
         fsb_host::set_error("fsb_spmm_csr: merge plan does not match the matrix");
         return FSB_ERR_INVALID;

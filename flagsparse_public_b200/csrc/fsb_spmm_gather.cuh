@@ -325,7 +325,7 @@ int launch_gather(const fsb_csr* Am, const V* val, const I* col, const P* ptr, c
     constexpr int kMaxBytes = (int)(sizeof(V) > sizeof(O) ? sizeof(V) : sizeof(O));
     constexpr int VW = 16 / kMaxBytes >= 1 ? 16 / kMaxBytes : 1;
     const int64_t n_units = plan->n_units;
-    if (plan->items_per_unit < 1 || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
+    if (plan->items_per_unit < 1 || plan->items_per_unit > kMaxItemsPerUnit || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
         !plan->unit_coords || plan->row_cap > 0) {
         fsb_host::set_error("fsb_spmm_csr: gather plan does not match the matrix");
         return FSB_ERR_INVALID;

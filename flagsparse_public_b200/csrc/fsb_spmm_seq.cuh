@@ -303,7 +303,7 @@ int launch_seq(const fsb_csr* Am, const V* val, const I* col, const P* ptr, cons
                int64_t n_dense, O* C, int64_t ldc, const fsb_plan* plan, void* workspace, int64_t workspace_bytes,
                cudaStream_t st) {
     const int64_t n_units = plan->n_units;
-    if (plan->items_per_unit < 1 || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
+    if (plan->items_per_unit < 1 || plan->items_per_unit > kMaxItemsPerUnit || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
         !plan->unit_coords || plan->row_cap > 0) {
         fsb_host::set_error("fsb_spmm_csr: seq plan does not match the matrix");
         return FSB_ERR_INVALID;

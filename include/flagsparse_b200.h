@@ -91,7 +91,8 @@ typedef struct fsb_csr {
 typedef struct fsb_plan {
     int32_t algo;            /* FSB_ALGO_ROWS / FSB_ALGO_MERGE                     */
     int32_t lanes;           /* ROWS: lanes per row group, power of two in [1, 32] */
-    int32_t items_per_unit;  /* MERGE: path items (rows + nnz) per unit           */
+    int32_t items_per_unit;  /* merge-path plans: items (rows + nnz) per unit,
+                                1 .. 2^24 for SpMM                               */
     int32_t n_tile;          /* SpMM: dense columns per column tile, 0 = all       */
     int64_t n_units;         /* MERGE: number of units                             */
     const int64_t* unit_coords; /* MERGE: device array [(n_units + 1) * 2] of

@@ -56,3 +56,19 @@ def test_invalid_arguments_rejected_without_launch():
     assert b"null" in lib.fsb_last_error()
     rc = lib.fsb_merge_partition(None, nat.FSB_I64, 10, 10, 128, 0, None, 1, None)
     assert rc == nat.FSB_ERR_INVALID
+
+
+def test_spmm_rejects_oversized_units_on_the_host():
+    """The launchers check items_per_unit before touching the device."""
+    import torch
+    lib = nat.library()
+    for algo in (nat.ALGO_MERGE, nat.ALGO_SEQ):
+        csr = nat.FsbCsr()
+        csr.value_dtype, csr.index_dtype, csr.ptr_dtype, csr.row_map_dtype = nat.FSB_F32, nat.FSB_I32, nat.FSB_I64, nat.FSB_I32
+        csr.n_rows, csr.n_cols, csr.nnz = 4, 4, 4
+        csr.values = csr.col_idx = csr.row_ptr = 16  # never dereferenced: rejected first
+        plan = nat.make_plan(algo, items_per_unit=(1 << 24) + 1, n_units=1, coords=None)
+        plan.unit_coords = 16
+        rc = lib.fsb_spmm_csr(ctypes.byref(csr), 16, 8, 8, 16, 8, nat.FSB_F32, nat.ACC_NATIVE, ctypes.byref(plan), 16,
+                              1 << 20, None)
+        assert rc == nat.FSB_ERR_INVALID, (algo, rc)
