@@ -235,6 +235,24 @@ def chosen_spmm_plan(stats, data, indices, indptr, n_rows, n_cols, B, C, acc_mod
     return plan
 
 
+def sorted_keys_to_offsets(keys, n_bins):
+    """int64 offsets[0 .. n_bins] of nondecreasing keys in [0, n_bins):
+    cumsum(bincount(keys)) computed without reading anything back to the host
+    (fsb_sorted_keys_to_offsets on CUDA tensors; a plain bincount on CPU)."""
+    n_bins = int(n_bins)
+    if not keys.is_cuda:
+        out = torch.zeros(n_bins + 1, dtype=torch.int64, device=keys.device)
+        if keys.numel():
+            out[1:] = torch.cumsum(torch.bincount(keys.to(torch.int64), minlength=n_bins), dim=0)
+        return out
+    keys = keys.contiguous()
+    out = torch.empty(n_bins + 1, dtype=torch.int64, device=keys.device)
+    rc = nat.library().fsb_sorted_keys_to_offsets(nat.ptr(keys), nat.dtype_code(keys.dtype), keys.numel(), n_bins,
+                                                  nat.ptr(out), nat.stream_handle(keys.device))
+    nat.check(rc, "fsb_sorted_keys_to_offsets")
+    return out
+
+
 def _workspace(is_spmm, cm, n_dense, acc_mode, out_code, cp, device):
     lib = nat.library()
     nbytes = int(lib.fsb_workspace_bytes(int(is_spmm), cm, int(n_dense), int(acc_mode), int(out_code), cp))

@@ -169,3 +169,37 @@ extern "C" int fsb_spmm_coo_atomic(const void* values, const void* row, const vo
         });
     });
 }
+
+namespace fsb {
+// offsets[b] = number of keys < b, for b in [0, n_bins]: a lower-bound search
+// of each bin boundary in the sorted keys (thread per boundary).
+template <class K>
+__global__ void k_sorted_keys_to_offsets(const K* __restrict__ keys, int64_t n, int64_t n_bins,
+                                         int64_t* __restrict__ offsets) {
+    const int64_t b = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (b > n_bins) return;
+    int64_t lo = 0, hi = n;
+    while (lo < hi) {
+        const int64_t mid = lo + ((hi - lo) >> 1);
+        if (idx(keys[mid]) < b) lo = mid + 1;
+        else hi = mid;
+    }
+    offsets[b] = lo;
+}
+}  // namespace fsb
+
+extern "C" int fsb_sorted_keys_to_offsets(const void* keys, int key_dtype, int64_t n, int64_t n_bins,
+                                          int64_t* offsets, void* stream) {
+    if (n < 0 || n_bins < 0 || !offsets || (n > 0 && !keys)) {
+        fsb_host::set_error("fsb_sorted_keys_to_offsets: bad arguments");
+        return FSB_ERR_INVALID;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return fsb::dispatch_idx(key_dtype, [&](auto tk) -> int {
+        using K = typename decltype(tk)::type;
+        const int64_t threads = n_bins + 1;
+        fsb::k_sorted_keys_to_offsets<K><<<(unsigned)fsb::ceil_div(threads, (int64_t)256), 256, 0, st>>>(
+            static_cast<const K*>(keys), n, n_bins, offsets);
+        return fsb_host::check_launch("k_sorted_keys_to_offsets");
+    });
+}

@@ -209,8 +209,7 @@ def _transpose_csr_for_spmv(data, indices, indptr, shape):
                                       output_size=nnz)
     cols = indices.to(torch.int64)
     sorted_cols, order = torch.sort(cols, stable=True)
-    t_indptr = torch.zeros(n_cols + 1, dtype=torch.int64, device=device)
-    t_indptr[1:] = torch.cumsum(torch.bincount(sorted_cols, minlength=n_cols), dim=0)
+    t_indptr = _plan.sorted_keys_to_offsets(sorted_cols, n_cols)
     return (
         data[order].contiguous(),
         row_ids[order].to(out_index_dtype).contiguous(),
@@ -580,8 +579,9 @@ def coo_to_csr_for_spmv(data, row, col, shape, assume_sorted=False):
         key = row64 * max(1, n_cols) + col64
         _, order = torch.sort(key, stable=True)
         row_s, col_s, data_s = row64[order], col64[order], data[order]
-    indptr = torch.zeros(n_rows + 1, dtype=torch.int64, device=data.device)
-    indptr[1:] = torch.cumsum(torch.bincount(row_s, minlength=n_rows), dim=0)
+    # row offsets on the device, no host read: with assume_sorted the whole
+    # conversion can be captured in a CUDA graph
+    indptr = _plan.sorted_keys_to_offsets(row_s, n_rows)
     return data_s, col_s.to(torch.int32), indptr
 
 

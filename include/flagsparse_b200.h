@@ -190,6 +190,15 @@ int fsb_spmm_coo_atomic(const void* values, const void* row, const void* col,
                         const void* B, int64_t ldb, int64_t n_dense, void* C,
                         int64_t ldc, int acc_dtype, void* stream);
 
+/* offsets[b] = number of keys below b for b = 0 .. n_bins (n_bins + 1
+ * entries) from nondecreasing keys in [0, n_bins): CSR row offsets of sorted
+ * COO rows, column offsets of a transpose.  No host synchronisation (can be
+ * captured in a CUDA graph); equals cumsum(bincount(keys)).  Replaces the
+ * bincount + cumsum of coo_to_csr_for_spmv (spmv_csr.py:885-909) and
+ * _transpose_csr_for_spmv (spmv_csr.py:456-494).                          */
+int fsb_sorted_keys_to_offsets(const void* keys, int key_dtype, int64_t n,
+                               int64_t n_bins, int64_t* offsets, void* stream);
+
 /* ---- block-sparse SpMM on the tensor cores ----------------------------- *
  * C (float32, n_rows x n_dense, row stride ldc) = A B for A in BSR form with
  * dense 16 x 16 blocks: block_values[n_blocks][16][16] (row-major blocks,

@@ -457,3 +457,26 @@ def test_spmm_opt_type_checks():
     prepared = fs.prepare_spmm_csr_opt(d.half(), i, p, (2, 2))
     with pytest.raises(TypeError, match="only supports float32 and float64"):
         fs.flagsparse_spmm_csr_opt(B=B.half(), prepared=prepared)
+
+
+def test_sorted_coo_to_csr_is_graph_capturable():
+    """With assume_sorted the COO -> CSR conversion reads nothing back to the
+    host, so it can be captured in a CUDA graph; the replay equals eager mode
+    and cumsum(bincount)."""
+    from flagsparse_public_b200.sparse_operations.spmv_csr import coo_to_csr_for_spmv
+    from flagsparse_public_b200 import synthetic
+    data, indices, indptr, shape = synthetic.zipf_powerlaw(5000, 4000, mean=6.0, cap=400, seed=11, device="cuda")
+    row = torch.repeat_interleave(torch.arange(shape[0], device="cuda"), indptr[1:] - indptr[:-1]).to(torch.int32)
+    eager = coo_to_csr_for_spmv(data, row, indices, shape, assume_sorted=True)
+    assert torch.equal(eager[2], indptr)
+    coo_to_csr_for_spmv(data, row, indices, shape, assume_sorted=True)  # warm-up outside capture
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        captured = coo_to_csr_for_spmv(data, row, indices, shape, assume_sorted=True)
+    g.replay()
+    torch.cuda.synchronize()
+    assert all(torch.equal(a, b) for a, b in zip(eager, captured))
+    ref = torch.zeros(shape[0] + 1, dtype=torch.int64, device="cuda")
+    ref[1:] = torch.cumsum(torch.bincount(row.long(), minlength=shape[0]), 0)
+    assert torch.equal(captured[2], ref)
