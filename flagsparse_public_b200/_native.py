@@ -117,8 +117,8 @@ _SIGNATURES = {
     "fsb_bsr_spmm_tc": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
-         ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
-         ctypes.c_int, ctypes.c_void_p],
+         ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_int64, ctypes.c_int, ctypes.c_void_p],
     ),
     "fsb_sorted_keys_to_offsets": (
         ctypes.c_int,

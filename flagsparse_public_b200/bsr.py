@@ -111,7 +111,8 @@ def flagsparse_spmm_bsr(block_values=None, block_col=None, block_row_ptr=None, B
     def launch(mode):
         return lib.fsb_bsr_spmm_tc(nat.ptr(p.block_values), nat.dtype_code(p.block_values.dtype),
                                    nat.ptr(p.block_col), nat.dtype_code(p.block_col.dtype), nat.ptr(p.block_row_ptr),
-                                   nat.dtype_code(p.block_row_ptr.dtype), p.shape[0], p.shape[1], nat.ptr(B),
+                                   nat.dtype_code(p.block_row_ptr.dtype), p.shape[0], p.shape[1], p.n_blocks,
+                                   nat.ptr(B),
                                    int(B.stride(0)), n_dense, nat.ptr(C), int(C.stride(0)), mode,
                                    nat.stream_handle(B.device))
 

@@ -22,8 +22,11 @@
 // Two stagings of the B slices:
 //   * k_bsr_spmm_tma (default): the Tensor Memory Accelerator loads each
 //     slice as two 64-column x 16-row boxes of a 2-D tensor map over B
-//     (128-byte swizzle) into a 4-stage ring, one thread keeping three blocks
-//     in flight ahead of the MMAs (SWIZZLE_128B MN-major operand);
+//     (128-byte swizzle; SWIZZLE_128B MN-major operand) and each block as one
+//     box of a 5-D tensor map over the block array that lands in the K-major
+//     core-matrix order, into a 4-stage ring; one thread runs the pipeline
+//     (loads three blocks ahead, MMA, commit, refill) with no CTA barrier per
+//     block;
 //   * k_bsr_spmm_tc: the CTA's threads copy the slice with 16-byte loads into
 //     two alternating stages (SWIZZLE_NONE MN-major operand).
 //
@@ -261,14 +264,28 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, int c4, uint32_t bar) {
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
+        "%6}], [%7];" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(0), "r"(0), "r"(c4), "r"(bar)
+        : "memory");
+}
+
+// One thread runs the pipeline: TMA loads of the B slice (two 64 x 16 boxes
+// of bmap) and of the 16 x 16 block (one box of amap, a 5-D view of the
+// block array whose box lands in the K-major core-matrix order) into a
+// 4-stage ring, the MMA once a stage is full, its commit to the stage's
+// empty barrier, and the refill of the stage three blocks ahead.  No CTA
+// barrier per block: the other warps wait for the last commit only.
 template <class V, class I, class P>
 __global__ void __launch_bounds__(kThreads)
-k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const V* __restrict__ blocks, const I* __restrict__ bcol,
-               const P* __restrict__ bptr, int64_t n_rows, int64_t n_dense, float* __restrict__ C, int64_t ldc,
-               int* __restrict__ err) {
+k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const __grid_constant__ CUtensorMap amap,
+               const I* __restrict__ bcol, const P* __restrict__ bptr, int64_t n_rows, int64_t n_dense,
+               float* __restrict__ C, int64_t ldc, int* __restrict__ err) {
     constexpr bool kBf16 = std::is_same<V, __nv_bfloat16>::value;
     constexpr int S = kTmaStages;
-    constexpr uint32_t kSliceBytes = 2 * kTmaBoxBytes;
+    constexpr uint32_t kStageTx = 2 * kTmaBoxBytes + kBStageBytes;
     __shared__ __align__(1024) unsigned char sa[S][2 * kTmaBoxBytes];
     __shared__ __align__(128) unsigned char sb[S][kBStageBytes];
     __shared__ __align__(8) uint64_t full[S], empty[S];
@@ -281,14 +298,14 @@ k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const V* __restrict__ b
     const int64_t b0 = idx(bptr[r]), b1 = idx(bptr[r + 1]);
     const int nb = (int)(b1 - b0);
 
-    auto issue = [&](int b) {  // thread 0: slice of block b into stage b % S
+    auto issue = [&](int b) {  // thread 0: block b's operands into stage b % S
         const int s = b % S;
         const uint32_t bar = smem_u32(&full[s]);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kSliceBytes)
-                     : "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kStageTx) : "memory");
         const int y = (int)(idx(bcol[b0 + b]) * 16);
         tma_load_2d(smem_u32(&sa[s][0]), &bmap, (int)c0, y, bar);
         tma_load_2d(smem_u32(&sa[s][kTmaBoxBytes]), &bmap, (int)c0 + kTmaBoxCols, y, bar);
+        tma_load_5d(smem_u32(&sb[s][0]), &amap, (int)(b0 + b), bar);
     };
 
     if (tid == 0) {
@@ -311,72 +328,57 @@ k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const V* __restrict__ b
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_slot;
     constexpr uint32_t idesc = instr_desc<kBf16>();
-    if (tid == 0)
-        for (int b = 0; b < nb && b < S; ++b) issue(b);
 
-    int issued = nb < S ? nb : S;  // meaningful in thread 0 only
-    bool failed = false;
-    for (int b = 0; b < nb; ++b) {
-        const int s = b % S;
-        // the block's 16 x 16 values, K-major: (n, k) at (n % 8) * 16 +
-        // (k % 8) * 2 + (n / 8) * 256 + (k / 8) * 128.  Stage s was freed
-        // by thread 0's wait on empty[s] before it refilled the stage, which
-        // precedes this iteration's barrier.
-        if (tid < 32) {
-            const int n = tid >> 1, kc = tid & 1;
-            const uint4 v = ld_vec16(blocks + (b0 + b) * 256 + n * 16 + kc * 8);
-            *reinterpret_cast<uint4*>(&sb[s][(n & 7) * 16 + (n >> 3) * 256 + kc * 128]) = v;
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        if (__syncthreads_or(fail_flag)) {
-            failed = true;
-            break;
-        }
-        if (tid == 0) {
+    if (tid == 0) {
+        int issued = 0;
+        for (; issued < nb && issued < S; ++issued) issue(issued);
+        for (int b = 0; b < nb; ++b) {
+            const int s = b % S;
             if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((b / S) & 1))) {
                 fail_flag = 1;
-            } else {
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                // A: two 64-column groups 2 KB apart (LBO), 8-row groups 1 KB apart (SBO)
-                const uint64_t adesc = smem_desc_sw128(smem_u32(&sa[s][0]), kTmaBoxBytes, 1024);
-                const uint64_t bdesc = smem_desc(smem_u32(&sb[s][0]), 128, 256);
-                const uint32_t accumulate = b > 0 ? 1u : 0u;
-                const uint32_t zero = 0;
-                asm volatile(
-                    "{\n\t.reg .pred p;\n\t"
-                    "setp.ne.b32 p, %4, 0;\n\t"
-                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-                    "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(zero), "r"(zero), "r"(zero),
-                    "r"(zero)
-                    : "memory");
-                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                                 smem_u32(&empty[s]))
-                             : "memory");
-                if (b + S < nb) {
-                    // refill stage s with block b + S once this MMA has read it
-                    if (!mbar_wait(smem_u32(&empty[s]), (uint32_t)((b / S) & 1))) {
-                        fail_flag = 1;
-                    } else {
-                        issue(b + S);
-                        ++issued;
-                    }
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            // A: two 64-column groups 2 KB apart (LBO), 8-row groups 1 KB apart (SBO)
+            const uint64_t adesc = smem_desc_sw128(smem_u32(&sa[s][0]), kTmaBoxBytes, 1024);
+            const uint64_t bdesc = smem_desc(smem_u32(&sb[s][0]), 128, 256);
+            const uint32_t accumulate = b > 0 ? 1u : 0u;
+            const uint32_t zero = 0;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
+                "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(zero), "r"(zero), "r"(zero), "r"(zero)
+                : "memory");
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&empty[s]))
+                         : "memory");
+            if (b + S < nb) {
+                if (!mbar_wait(smem_u32(&empty[s]), (uint32_t)((b / S) & 1))) {
+                    fail_flag = 1;
+                    break;
                 }
+                issue(b + S);
+                ++issued;
+            }
+        }
+        if (fail_flag) {
+            // drain (bounded) what is still in flight before TMEM and the ring go away
+            for (int b = issued > S ? issued - S : 0; b < issued; ++b) {
+                mbar_wait(smem_u32(&full[b % S]), (uint32_t)((b / S) & 1));
+                mbar_wait(smem_u32(&empty[b % S]), (uint32_t)((b / S) & 1));
             }
         }
     }
-    if (nb > 0 && !failed) {
+    // everyone: the last MMA's commit (all earlier MMAs complete before it)
+    bool ok = true;
+    if (nb > 0) {
         const int last = nb - 1;
-        const bool ok = mbar_wait(smem_u32(&empty[last % S]), (uint32_t)((last / S) & 1));
-        failed = __syncthreads_or(!ok || fail_flag) != 0;
+        ok = mbar_wait(smem_u32(&empty[last % S]), (uint32_t)((last / S) & 1));
     }
+    const bool failed = __syncthreads_or(!ok || fail_flag) != 0;
     if (failed) {
-        if (tid == 0) {
-            atomicExch(err, FSB_ERR_TIMEOUT);
-            // drain (bounded) the copies and MMAs this CTA started
-            for (int b = 0; b < issued; ++b) mbar_wait(smem_u32(&full[b % S]), (uint32_t)((b / S) & 1));
-            for (int b = issued > S ? issued - S : 0; b < issued; ++b)
-                mbar_wait(smem_u32(&empty[b % S]), (uint32_t)((b / S) & 1));
-        }
+        if (tid == 0) atomicExch(err, FSB_ERR_TIMEOUT);
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         uint32_t d[16];
@@ -443,18 +445,36 @@ static bool encode_b_map(CUtensorMap* map, int value_dtype, const void* B, int64
     return rc == CUDA_SUCCESS;
 }
 
+// 5-D tensor map over the block array: (8 values, 8 rows, 2 halves of a
+// row, 2 groups of 8 rows, block) with byte strides 32, 16, 256, 512; a box
+// {8, 8, 2, 2, 1} lands as element (n, k) at (n % 8) * 16 + (k % 8) * 2 +
+// (k / 8) * 128 + (n / 8) * 256, the K-major core-matrix order of a block.
+static bool encode_block_map(CUtensorMap* map, int value_dtype, const void* blocks, int64_t n_blocks) {
+    auto fn = encode_fn();
+    if (!fn || n_blocks < 1 || n_blocks >= 0x7fffffffLL) return false;
+    const cuuint64_t dims[5] = {8, 8, 2, 2, (cuuint64_t)n_blocks};
+    const cuuint64_t strides[4] = {32, 16, 256, 512};
+    const cuuint32_t box[5] = {8, 8, 2, 2, 1};
+    const cuuint32_t estr[5] = {1, 1, 1, 1, 1};
+    const CUresult rc = fn(map, value_dtype == FSB_BF16 ? CU_TENSOR_MAP_DATA_TYPE_BFLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT16,
+                           5, const_cast<void*>(blocks), dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                           CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_NONE,
+                           CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return rc == CUDA_SUCCESS;
+}
+
 }  // namespace bsr
 }  // namespace fsb
 
 extern "C" int fsb_bsr_spmm_tc(const void* block_values, int value_dtype, const void* block_col, int index_dtype,
                                const void* block_row_ptr, int ptr_dtype, int64_t n_rows, int64_t n_cols,
-                               const void* B, int64_t ldb, int64_t n_dense, float* C, int64_t ldc, int staging,
-                               void* stream) {
+                               int64_t n_blocks, const void* B, int64_t ldb, int64_t n_dense, float* C, int64_t ldc,
+                               int staging, void* stream) {
     if (value_dtype != FSB_BF16 && value_dtype != FSB_F16) {
         fsb_host::set_error("fsb_bsr_spmm_tc: values and B must be bfloat16 or float16");
         return FSB_ERR_UNSUPPORTED;
     }
-    if (n_rows < 0 || n_cols < 0 || n_dense < 0 || ldb < n_dense || ldc < n_dense) {
+    if (n_rows < 0 || n_cols < 0 || n_blocks < 0 || n_dense < 0 || ldb < n_dense || ldc < n_dense) {
         fsb_host::set_error("fsb_bsr_spmm_tc: bad sizes");
         return FSB_ERR_INVALID;
     }
@@ -485,25 +505,28 @@ extern "C" int fsb_bsr_spmm_tc(const void* block_values, int value_dtype, const 
     }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     dim3 g((unsigned)n_block_rows, (unsigned)tiles);
-    CUtensorMap bmap;
+    CUtensorMap bmap, amap;
     if (staging == FSB_BSR_STAGE_TMA) {
         if (n_cols >= 0x7fffffffLL || n_dense >= 0x7fffffffLL ||
-            !fsb::bsr::encode_b_map(&bmap, value_dtype, B, n_cols, ldb, n_dense)) {
-            fsb_host::set_error("fsb_bsr_spmm_tc: no tensor map can be encoded for B (use FSB_BSR_STAGE_THREADS)");
+            !fsb::bsr::encode_b_map(&bmap, value_dtype, B, n_cols, ldb, n_dense) ||
+            (n_blocks > 0 && !fsb::bsr::encode_block_map(&amap, value_dtype, block_values, n_blocks))) {
+            fsb_host::set_error("fsb_bsr_spmm_tc: no tensor map can be encoded for B or the blocks "
+                                "(use FSB_BSR_STAGE_THREADS)");
             return FSB_ERR_UNSUPPORTED;
         }
+        if (n_blocks == 0) amap = bmap;  // never read: no block row holds a block
         return fsb::dispatch_idx(index_dtype, [&](auto ti) -> int {
             using I = typename decltype(ti)::type;
             return fsb::dispatch_idx(ptr_dtype, [&](auto tp) -> int {
                 using P = typename decltype(tp)::type;
                 if (value_dtype == FSB_BF16)
                     fsb::bsr::k_bsr_spmm_tma<__nv_bfloat16, I, P><<<g, fsb::bsr::kThreads, 0, st>>>(
-                        bmap, static_cast<const __nv_bfloat16*>(block_values), static_cast<const I*>(block_col),
-                        static_cast<const P*>(block_row_ptr), n_rows, n_dense, C, ldc, err);
+                        bmap, amap, static_cast<const I*>(block_col), static_cast<const P*>(block_row_ptr), n_rows,
+                        n_dense, C, ldc, err);
                 else
                     fsb::bsr::k_bsr_spmm_tma<__half, I, P><<<g, fsb::bsr::kThreads, 0, st>>>(
-                        bmap, static_cast<const __half*>(block_values), static_cast<const I*>(block_col),
-                        static_cast<const P*>(block_row_ptr), n_rows, n_dense, C, ldc, err);
+                        bmap, amap, static_cast<const I*>(block_col), static_cast<const P*>(block_row_ptr), n_rows,
+                        n_dense, C, ldc, err);
                 return fsb_host::check_launch("k_bsr_spmm_tma");
             });
         });

@@ -207,18 +207,20 @@ int fsb_sorted_keys_to_offsets(const void* keys, int key_dtype, int64_t n,
  * stride ldb) has the same 16-bit type, is 16-byte aligned, with ldb and
  * n_dense multiples of 8.  tcgen05.mma (kind::f16, fp32 accumulation in
  * tensor memory), one MMA of 128 x 16 x 16 per stored block and 128-column
- * tile.  staging: FSB_BSR_STAGE_TMA stages the B slices with the Tensor
- * Memory Accelerator (2-D tensor map, 4-stage ring; FSB_ERR_UNSUPPORTED
- * when no tensor map can be encoded for B), FSB_BSR_STAGE_THREADS with the
- * CTA's threads.  No FlagSparse counterpart: FlagSparse runs
+ * tile; n_blocks = block_row_ptr's last entry.  staging:
+ * FSB_BSR_STAGE_TMA stages B slices and blocks with the Tensor Memory
+ * Accelerator (tensor maps, 4-stage ring run by one thread;
+ * FSB_ERR_UNSUPPORTED when no tensor map can be encoded),
+ * FSB_BSR_STAGE_THREADS with the CTA's threads.  No FlagSparse counterpart: FlagSparse runs
  * block-structured matrices through its CSR SpMM (spmm_csr.py:2088-2157).  */
 #define FSB_BSR_STAGE_TMA     0
 #define FSB_BSR_STAGE_THREADS 1
 int fsb_bsr_spmm_tc(const void* block_values, int value_dtype,
                     const void* block_col, int index_dtype,
                     const void* block_row_ptr, int ptr_dtype, int64_t n_rows,
-                    int64_t n_cols, const void* B, int64_t ldb, int64_t n_dense,
-                    float* C, int64_t ldc, int staging, void* stream);
+                    int64_t n_cols, int64_t n_blocks, const void* B,
+                    int64_t ldb, int64_t n_dense, float* C, int64_t ldc,
+                    int staging, void* stream);
 
 /* ---- SDDMM ------------------------------------------------------------- *
  * out[p] = alpha * dot(x[row_ids[p]], y[col_idx[p]]) + beta * data[p] for
