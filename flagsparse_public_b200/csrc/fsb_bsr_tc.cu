@@ -245,7 +245,7 @@ k_bsr_spmm_tc(const V* __restrict__ blocks, const I* __restrict__ bcol, const P*
     }
 }
 
-constexpr int kTmaStages = 4;
+constexpr int kTmaStages = 3;
 constexpr int kTmaBoxCols = 64;                      // 128 bytes of 16-bit values
 constexpr int kTmaBoxBytes = kTmaBoxCols * 16 * 2;  // 2 KB per box, 2 boxes per slice
 
@@ -279,7 +279,7 @@ __device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map
 // empty barrier, and the refill of the stage three blocks ahead.  No CTA
 // barrier per block: the other warps wait for the last commit only.
 template <class V, class I, class P>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kThreads, 16)
 k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const __grid_constant__ CUtensorMap amap,
                const I* __restrict__ bcol, const P* __restrict__ bptr, int64_t n_rows, int64_t n_dense,
                float* __restrict__ C, int64_t ldc, int* __restrict__ err) {
@@ -381,28 +381,29 @@ k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const __grid_constant__
         if (tid == 0) atomicExch(err, FSB_ERR_TIMEOUT);
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        uint32_t d[16];
-        if (nb > 0) {
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
-                "%13, %14, %15}, [%16];"
-                : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7]),
-                  "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]),
-                  "=r"(d[15])
-                : "r"(taddr)
-                : "memory");
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-        } else {
-#pragma unroll
-            for (int n = 0; n < 16; ++n) d[n] = 0u;
-        }
+        // two 8-column halves keep the read-out at 8 registers
         const int m = warp * 32 + lane;
-        if (m < cols) {
 #pragma unroll
-            for (int n = 0; n < 16; ++n) {
-                const int64_t row = r * 16 + n;
-                if (row < n_rows) __stcs(C + row * ldc + c0 + m, __uint_as_float(d[n]));
+        for (int h = 0; h < 2; ++h) {
+            uint32_t d[8];
+            if (nb > 0) {
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * 8);
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                    : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7])
+                    : "r"(taddr)
+                    : "memory");
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            } else {
+#pragma unroll
+                for (int n = 0; n < 8; ++n) d[n] = 0u;
+            }
+            if (m < cols) {
+#pragma unroll
+                for (int n = 0; n < 8; ++n) {
+                    const int64_t row = r * 16 + h * 8 + n;
+                    if (row < n_rows) __stcs(C + row * ldc + c0 + m, __uint_as_float(d[n]));
+                }
             }
         }
     }
