@@ -56,7 +56,7 @@ def parse_args(argv=None):
                     help="only warm-up + timed device steps (for a profiler launch list)")
     ap.add_argument("--plan", default=None,
                     help="force the chosen-form plan: rows:<lanes>[:<n_tile>] | merge:<items>:<snap> | "
-                         "flat|gather|seq:<items>:<snap>[:<n_tile>]")
+                         "flat|gather|seq:<items>:<snap>[:<n_tile>] | g4:<items>[:<snap>[:<n_tile>]]")
     return ap.parse_args(argv)
 
 
@@ -903,6 +903,9 @@ def parse_plan(text):
     kind, nums = parts[0], [int(v) for v in parts[1:]]
     if kind == "rows":
         return _plan.KernelPlan(nat.ALGO_ROWS, lanes=nums[0], n_tile=nums[1] if len(nums) > 1 else 0)
+    if kind == "g4":
+        return _plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=nums[0], snap=nums[1] if len(nums) > 1 else 0,
+                                n_tile=nums[2] if len(nums) > 2 else 0, flags=nat.PLAN_TMA_GATHER)
     algo = {"merge": nat.ALGO_MERGE, "flat": nat.ALGO_FLAT, "gather": nat.ALGO_GATHER, "seq": nat.ALGO_SEQ}[kind]
     return _plan.KernelPlan(algo, items_per_unit=nums[0], snap=nums[1] if len(nums) > 1 else 0,
                             n_tile=nums[2] if len(nums) > 2 else 0)

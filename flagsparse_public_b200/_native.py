@@ -27,6 +27,7 @@ FSB_ERR_LIMIT = -6
 FSB_F16, FSB_BF16, FSB_F32, FSB_F64, FSB_C64, FSB_C128, FSB_I32, FSB_I64 = range(8)
 ACC_NATIVE, ACC_WIDE, ACC_COMP = 0, 1, 2
 ALGO_ROWS, ALGO_MERGE, ALGO_FLAT, ALGO_GATHER, ALGO_SEQ = 0, 1, 2, 3, 4
+PLAN_TMA_GATHER = 1  # fsb_plan.flags: SEQ with B rows staged by TMA tile::gather4
 BSR_STAGE_TMA, BSR_STAGE_THREADS = 0, 1
 
 _DTYPE_CODES = {

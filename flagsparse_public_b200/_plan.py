@@ -64,10 +64,10 @@ class KernelPlan:
     """One launch configuration of fsb_spmv_csr / fsb_spmm_csr."""
 
     __slots__ = ("algo", "lanes", "items_per_unit", "n_tile", "snap", "coords", "n_units", "row_cap",
-                 "comp_threshold", "fallback_ok", "grid_blocks")
+                 "comp_threshold", "fallback_ok", "grid_blocks", "flags")
 
     def __init__(self, algo, lanes=32, items_per_unit=0, n_tile=0, snap=0, row_cap=0, comp_threshold=0,
-                 fallback_ok=False, grid_blocks=0):
+                 fallback_ok=False, grid_blocks=0, flags=0):
         self.algo = int(algo)
         self.lanes = int(lanes)
         self.items_per_unit = int(items_per_unit)
@@ -79,6 +79,7 @@ class KernelPlan:
         self.comp_threshold = int(comp_threshold)
         self.fallback_ok = bool(fallback_ok)
         self.grid_blocks = int(grid_blocks)
+        self.flags = int(flags)
 
     def as_flat(self):
         """The register-staged flat plan over the same merge-path units."""
@@ -88,7 +89,7 @@ class KernelPlan:
         return p
 
     def key(self):
-        return (self.algo, self.lanes, self.items_per_unit, self.n_tile, self.snap, self.grid_blocks)
+        return (self.algo, self.lanes, self.items_per_unit, self.n_tile, self.snap, self.grid_blocks, self.flags)
 
     def describe(self):
         if self.algo == nat.ALGO_ROWS:
@@ -96,6 +97,8 @@ class KernelPlan:
             return {"kind": kind, "lanes": self.lanes, "n_tile": self.n_tile}
         kind = {nat.ALGO_MERGE: "merge_path", nat.ALGO_FLAT: "merge_path_flat",
                 nat.ALGO_GATHER: "merge_path_tma_gather", nat.ALGO_SEQ: "merge_path_seq"}[self.algo]
+        if self.algo == nat.ALGO_SEQ and self.flags & nat.PLAN_TMA_GATHER:
+            kind = "merge_path_seq_gather4"
         d = {"kind": kind, "items_per_unit": self.items_per_unit, "n_tile": self.n_tile,
              "snap": self.snap, "n_units": self.n_units}
         if self.grid_blocks:
@@ -104,7 +107,7 @@ class KernelPlan:
 
     def copy(self):
         p = KernelPlan(self.algo, self.lanes, self.items_per_unit, self.n_tile, self.snap, self.row_cap,
-                       self.comp_threshold, self.fallback_ok, self.grid_blocks)
+                       self.comp_threshold, self.fallback_ok, self.grid_blocks, self.flags)
         return p
 
     def ensure_coords(self, row_ptr, n_rows, nnz):
@@ -125,7 +128,7 @@ class KernelPlan:
     def c_plan(self):
         return nat.make_plan(self.algo, lanes=self.lanes, items_per_unit=self.items_per_unit, n_tile=self.n_tile,
                              coords=self.coords, n_units=self.n_units, row_cap=self.row_cap,
-                             comp_threshold=self.comp_threshold, grid_blocks=self.grid_blocks)
+                             comp_threshold=self.comp_threshold, grid_blocks=self.grid_blocks, flags=self.flags)
 
 
 def _pow2_clamp(v, lo, hi):
@@ -296,12 +299,42 @@ def gather_supported(B, C, n_tile=0):
             and C.stride(0) % vw == 0 and n_dense % vw == 0)
 
 
+G4_WARPS_PER_SM = 12  # resident warps of the gather4 SpMM (3 CTAs of 4 warps, 64 KB of rings each)
+
+
+def g4_items_per_unit(stats, units_per_warp=1):
+    """Merge-path unit size for the gather4 SpMM: (rows + nonzeros) over
+    units_per_warp units per resident warp (one pipeline fill per unit)."""
+    items = stats.n_rows + stats.nnz
+    return max(64, -(-items // (SM_COUNT * G4_WARPS_PER_SM * units_per_warp)))
+
+
+def g4_supported(values, B, C, acc_mode, n_cols):
+    """Whether the TMA gather4 form of the SEQ plan can run on these operands
+    (mirrors launch_g4 in fsb_spmm_g4.cuh): float32 / float16 / bfloat16
+    values with float accumulators, 16-byte aligned B rows, n_dense a multiple
+    of the 16-byte lane vector, C lane vectors aligned, n_cols below 2^31."""
+    if values.dtype not in (torch.float32, torch.float16, torch.bfloat16) or acc_mode == nat.ACC_COMP:
+        return False
+    vb, vc = B.element_size(), C.element_size()
+    vw = 16 // vb
+    n_dense = B.shape[1]
+    return (B.data_ptr() % 16 == 0 and (B.stride(0) * vb) % 16 == 0 and n_dense % vw == 0
+            and C.data_ptr() % min(16, vw * vc) == 0 and C.stride(0) % vw == 0 and int(n_cols) < 2 ** 31 - 1)
+
+
 def run_spmm(values, col_idx, row_ptr, n_rows, n_cols, B, C, acc_mode, plan, row_map=None):
     """C = A B through fsb_spmm_csr (B, C row-major with unit column stride)."""
     if plan.algo == nat.ALGO_GATHER and not gather_supported(B, C, plan.n_tile):
         if not plan.fallback_ok:
             raise ValueError("the TMA gather plan needs 16-byte aligned B and C rows")
         plan = plan.as_flat()
+    if plan.flags & nat.PLAN_TMA_GATHER and not g4_supported(values, B, C, acc_mode, n_cols):
+        if not plan.fallback_ok:
+            raise ValueError("the gather4 plan needs float32 / float16 / bfloat16 values, float accumulators and "
+                             "16-byte aligned B and C rows")
+        plan = plan.copy()
+        plan.flags &= ~nat.PLAN_TMA_GATHER
     plan.ensure_coords(row_ptr, n_rows, values.numel())
     n_dense = int(B.shape[1])
     cm = nat.make_csr(values, col_idx, row_ptr, n_rows, n_cols, row_map)

@@ -35,13 +35,9 @@
 // Every mbarrier wait is bounded (1 s, globaltimer); on expiry the kernel
 // records FSB_ERR_TIMEOUT in the device error word (fsb_device_error), waits
 // (bounded) for the MMA it issued, frees its TMEM and returns.
-#include <cuda.h>
-#include <cudaTypedefs.h>
-
-#include <mutex>
 #include <type_traits>
 
-#include "fsb_dispatch.cuh"
+#include "fsb_tma.cuh"
 
 namespace fsb {
 
@@ -54,7 +50,6 @@ constexpr int kM = 128;                         // dense columns per tile (MMA M
 constexpr int kAStageBytes = kM * 16 * 2;       // 16 B rows x 128 columns, 16-bit
 constexpr int kBStageBytes = 16 * 16 * 2;       // one 16 x 16 block
 constexpr int kTmemCols = 32;                   // allocation unit (16 used)
-constexpr unsigned long long kWaitNs = 1000000000ull;
 
 // Instruction descriptor, kind::f16: D f32 (bits 4-5 = 1), A and B 16-bit
 // (bits 7-9, 10-12: 0 = f16, 1 = bf16), A MN-major (bit 15), B K-major
@@ -73,32 +68,8 @@ __device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint3
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
 
-__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ unsigned long long now_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
-    return t;
-}
-__device__ __forceinline__ bool mbar_test(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}\n"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity), "r"(20000u)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the phase of the given parity; false when it gave up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-    if (mbar_test(bar, parity)) return true;
-    const unsigned long long t0 = now_ns();
-    while (!mbar_test(bar, parity))
-        if (now_ns() - t0 > kWaitNs) return false;
-    return true;
-}
+using tma::mbar_wait;
+using tma::smem_u32;
 
 template <class T>
 __device__ __forceinline__ uint4 ld_vec16(const T* p) {
@@ -415,25 +386,11 @@ k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const __grid_constant__
     }
 }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (once).
-static PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
-    static std::once_flag once;
-    static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
-    std::call_once(once, [] {
-        void* p = nullptr;
-        cudaDriverEntryPointQueryResult q;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
-    });
-    return fn;
-}
-
 // 2-D tensor map over B (columns innermost): 64 x 16 boxes, 128-byte swizzle,
 // zero fill outside the matrix.  False when it cannot be encoded.
 static bool encode_b_map(CUtensorMap* map, int value_dtype, const void* B, int64_t n_cols, int64_t ldb,
                          int64_t n_dense) {
-    auto fn = encode_fn();
+    auto fn = tma::encode_fn();
     if (!fn) return false;
     const cuuint64_t dims[2] = {(cuuint64_t)n_dense, (cuuint64_t)n_cols};
     const cuuint64_t strides[1] = {(cuuint64_t)ldb * 2};
@@ -451,7 +408,7 @@ static bool encode_b_map(CUtensorMap* map, int value_dtype, const void* B, int64
 // {8, 8, 2, 2, 1} lands as element (n, k) at (n % 8) * 16 + (k % 8) * 2 +
 // (k / 8) * 128 + (n / 8) * 256, the K-major core-matrix order of a block.
 static bool encode_block_map(CUtensorMap* map, int value_dtype, const void* blocks, int64_t n_blocks) {
-    auto fn = encode_fn();
+    auto fn = tma::encode_fn();
     if (!fn || n_blocks < 1 || n_blocks >= 0x7fffffffLL) return false;
     const cuuint64_t dims[5] = {8, 8, 2, 2, (cuuint64_t)n_blocks};
     const cuuint64_t strides[4] = {32, 16, 256, 512};

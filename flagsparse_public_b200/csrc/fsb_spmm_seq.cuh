@@ -22,7 +22,7 @@
 #pragma once
 #include <type_traits>
 
-#include "fsb_spmm_common.cuh"
+#include "fsb_spmm_g4.cuh"
 
 namespace fsb {
 
@@ -302,6 +302,11 @@ template <class V, class A, class O, class I, class P>
 int launch_seq(const fsb_csr* Am, const V* val, const I* col, const P* ptr, const I* rmap, const V* B, int64_t ldb,
                int64_t n_dense, O* C, int64_t ldc, const fsb_plan* plan, void* workspace, int64_t workspace_bytes,
                cudaStream_t st) {
+    // B rows staged by TMA gather4 (fsb_spmm_g4.cuh); a matrix without
+    // nonzeros gathers nothing and takes the plain kernel
+    if ((plan->flags & FSB_PLAN_TMA_GATHER) && Am->nnz > 0)
+        return launch_g4<V, A, O, I, P>(Am, val, col, ptr, rmap, B, ldb, n_dense, C, ldc, plan, workspace,
+                                        workspace_bytes, st);
     const int64_t n_units = plan->n_units;
     if (plan->items_per_unit < 1 || plan->items_per_unit > kMaxItemsPerUnit || n_units != ceil_div(Am->n_rows + Am->nnz, plan->items_per_unit) ||
         !plan->unit_coords || plan->row_cap > 0) {

@@ -69,6 +69,15 @@ extern "C" {
                               B rows gathered to registers, rows reduced
                               across sub-groups only at row ends            */
 
+/* ---- plan flags (fsb_plan.flags) ------------------------------------- */
+#define FSB_PLAN_TMA_GATHER 1  /* SEQ: B rows staged in a per-warp shared-memory
+                                  ring by TMA row gathers (tile::gather4, four
+                                  B rows per instruction), several stages ahead
+                                  of the multiply-adds; float32 / float16 /
+                                  bfloat16 values, float accumulators, 16-byte
+                                  aligned B and C rows, else
+                                  FSB_ERR_UNSUPPORTED                          */
+
 /* A CSR matrix (or a sorted COO matrix seen as row runs).
  * row_ptr has n_rows + 1 entries.  If row_map is non-null, row r of this
  * structure is written to output row row_map[row_ptr[r]] (COO row runs:
@@ -103,7 +112,7 @@ typedef struct fsb_plan {
                                 compensated (FlagSparse precision form: 4096)     */
     int32_t grid_blocks;     /* ROWS, SEQ: CTAs to launch (SEQ: a persistent grid
                                 striding over the units), 0 = automatic           */
-    int32_t flags;           /* reserved, 0                                         */
+    int32_t flags;           /* FSB_PLAN_* bits, 0 = none                          */
 } fsb_plan;
 
 int         fsb_abi_version(void);

@@ -161,6 +161,8 @@ def test_spmm_all_plans(pattern, n_dense, mode):
         C = torch.full((n_rows, n_dense), float("nan"), dtype=out_dtype, device=DEV)
         if plan.algo == nat.ALGO_GATHER and not _plan.gather_supported(Bd, C, plan.n_tile):
             continue
+        if plan.flags & nat.PLAN_TMA_GATHER and not _plan.g4_supported(d[0], Bd, C, acc, n_cols):
+            continue
         _plan.run_spmm(*d, n_rows, n_cols, Bd, C, acc, plan)
         err = scaled_error(C, exact, mag)
         assert err <= bound, (plan.describe(), err)
