@@ -256,6 +256,57 @@ def sorted_keys_to_offsets(keys, n_bins):
     return out
 
 
+def stable_sort(keys, key_bound=None):
+    """(sorted keys, int64 permutation) of a 1-D int32 / int64 tensor, equal
+    to ``torch.sort(keys, stable=True)``: fsb_stable_sort (LSD radix sort) on
+    CUDA tensors, torch on CPU.  ``key_bound``: an exclusive upper bound of
+    non-negative keys (fewer radix passes); None sorts the full signed width."""
+    if not keys.is_cuda:
+        return torch.sort(keys, stable=True)
+    keys = keys.contiguous()
+    n = keys.numel()
+    width = 32 if keys.dtype == torch.int32 else 64
+    if keys.dtype not in (torch.int32, torch.int64):
+        raise TypeError("stable_sort: keys must be int32 or int64")
+    bits = width if key_bound is None else min(width, max(1, (max(int(key_bound), 1) - 1).bit_length()))
+    out = torch.empty_like(keys)
+    order = torch.empty(n, dtype=torch.int64, device=keys.device)
+    if n == 0:
+        return out, order
+    lib = nat.library()
+    code = nat.dtype_code(keys.dtype)
+    nbytes = int(lib.fsb_sort_workspace_bytes(n, code, bits))
+    ws = torch.empty(max(nbytes, 1), dtype=torch.uint8, device=keys.device)
+    rc = lib.fsb_stable_sort(nat.ptr(keys), code, n, bits, nat.ptr(out), nat.ptr(order), nat.ptr(ws), nbytes,
+                             nat.stream_handle(keys.device))
+    nat.check(rc, "fsb_stable_sort")
+    return out, order
+
+
+def run_starts(sorted_keys, out_dtype):
+    """[0, start of every later run of equal keys ..., n] of sorted 1-D keys in
+    ``out_dtype`` (int32 / int64): fsb_run_starts on CUDA tensors (one host
+    read of the run count), the equivalent torch expression on CPU.  None for
+    no keys."""
+    n = sorted_keys.numel()
+    if n == 0:
+        return None
+    if not sorted_keys.is_cuda:
+        breaks = torch.nonzero(sorted_keys[1:] != sorted_keys[:-1], as_tuple=False).flatten().to(out_dtype) + 1
+        return torch.cat([torch.zeros(1, dtype=out_dtype), breaks, torch.tensor([n], dtype=out_dtype)])
+    keys = sorted_keys.contiguous()
+    lib = nat.library()
+    starts = torch.empty(n + 1, dtype=out_dtype, device=keys.device)
+    count = torch.empty(1, dtype=torch.int64, device=keys.device)
+    nbytes = int(lib.fsb_run_starts_workspace_bytes(n))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=keys.device)
+    rc = lib.fsb_run_starts(nat.ptr(keys), nat.dtype_code(keys.dtype), n, nat.ptr(starts),
+                            nat.dtype_code(out_dtype), nat.ptr(count), nat.ptr(ws), nbytes,
+                            nat.stream_handle(keys.device))
+    nat.check(rc, "fsb_run_starts")
+    return starts[: int(count.item())].clone()
+
+
 def _workspace(is_spmm, cm, n_dense, acc_mode, out_code, cp, device):
     lib = nat.library()
     nbytes = int(lib.fsb_workspace_bytes(int(is_spmm), cm, int(n_dense), int(acc_mode), int(out_code), cp))

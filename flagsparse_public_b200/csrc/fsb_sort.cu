@@ -1,0 +1,370 @@
+// fsb_sort.cu -- the integer prepare steps on the device: a stable LSD radix
+// sort of integer keys returning the permutation (the stable argsorts of
+// FlagSparse's prepare functions: the column sort of _transpose_csr_for_spmv,
+// spmv_csr.py:456-494; the (row, col) key sorts of coo_to_csr_for_spmv,
+// spmv_csr.py:885-909, _sort_coo_lex_inplace, spmv_coo.py:297-309 and
+// spmm_coo.py:21-32), and the starts of equal-key runs of sorted keys
+// (_seg_starts_from_sorted_rows, spmv_coo.py:312-327, spmm_coo.py:121-132).
+//
+// Radix sort: 8-bit digits, least significant first, one pass per digit of
+// the caller's key width (key_bits).  A pass is three kernels over tiles of
+// kTile keys:
+//   * k_sort_upsweep: per-tile digit histogram (warp-aggregated shared-memory
+//     counts), stored digit-major: hist[digit][tile];
+//   * k_scan_rows: one CTA per digit scans its row of tile counts in place
+//     (exclusive) and records the digit's total;
+//   * k_sort_downsweep: each tile scans the 256 totals for the digit starts,
+//     then ranks its keys in rounds of 256 (one per thread, in key order):
+//     __match_any_sync groups the warp's equal digits, per-warp digit counts
+//     in shared memory are prefixed over the warps by the thread that owns
+//     the digit, and the key and its permutation entry are written to
+//     digit start + tile prefix + rank.  Ranks follow key order inside the
+//     tile and tiles follow each other, so every pass is stable and the
+//     result equals a stable sort (torch.sort(stable=True)) bit for bit.
+// The permutation travels as 32-bit indices between passes and is written as
+// int64 by the last pass.  Keys of the full signed width are ordered through
+// their top bit flipped.  HBM bound: a pass reads the keys twice and the
+// permutation once and writes both.
+#include "fsb_dispatch.cuh"
+
+namespace fsb {
+namespace sort {
+
+constexpr int kThreads = 256;
+constexpr int kBins = 256;
+constexpr int kRounds = 16;
+constexpr int kTile = kThreads * kRounds;  // keys per tile
+constexpr int kWarps = kThreads / 32;
+
+// Inclusive scan of one value per thread over the CTA; *total receives the
+// CTA sum.  sums: kWarps shared words.  Contains __syncthreads.
+__device__ __forceinline__ uint32_t block_scan(uint32_t v, uint32_t* sums, uint32_t* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    if (lane == 31) sums[warp] = v;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kWarps ? sums[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < kWarps; o <<= 1) {
+            const uint32_t t = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += t;
+        }
+        if (lane < kWarps) sums[lane] = w;
+    }
+    __syncthreads();
+    const uint32_t add = warp > 0 ? sums[warp - 1] : 0u;
+    *total = sums[kWarps - 1];
+    __syncthreads();
+    return v + add;
+}
+
+template <class K>
+__device__ __forceinline__ int digit_of(K k, int shift, uint32_t mask) {
+    return (int)((uint32_t)(k >> shift) & mask);
+}
+
+template <class K>
+__global__ void __launch_bounds__(kThreads)
+k_sort_upsweep(const K* __restrict__ keys, int64_t n, K flip, int shift, uint32_t mask, uint32_t* __restrict__ hist,
+               int64_t n_tiles) {
+    __shared__ uint32_t h[kBins];
+    const int lane = threadIdx.x & 31;
+    h[threadIdx.x] = 0u;
+    __syncthreads();
+    const int64_t t0 = (int64_t)blockIdx.x * kTile;
+#pragma unroll 4
+    for (int r = 0; r < kRounds; ++r) {
+        const int64_t i = t0 + (int64_t)r * kThreads + threadIdx.x;
+        const int d = i < n ? digit_of<K>(keys[i] ^ flip, shift, mask) : kBins;
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        if (d < kBins && (peers & ((1u << lane) - 1u)) == 0u) atomicAdd(&h[d], (uint32_t)__popc(peers));
+    }
+    __syncthreads();
+    hist[(int64_t)threadIdx.x * n_tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+// One CTA per row: rows[b * len .. b * len + len) scanned in place
+// (exclusive); totals[b] = the row's sum.
+__global__ void __launch_bounds__(kThreads)
+k_scan_rows(uint32_t* __restrict__ rows, int64_t len, uint32_t* __restrict__ totals) {
+    __shared__ uint32_t sums[kWarps];
+    uint32_t* row = rows + (int64_t)blockIdx.x * len;
+    uint32_t carry = 0;
+    for (int64_t c0 = 0; c0 < len; c0 += (int64_t)kThreads * 4) {
+        uint32_t v[4], s = 0;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t i = c0 + (int64_t)threadIdx.x * 4 + j;
+            v[j] = i < len ? row[i] : 0u;
+            s += v[j];
+        }
+        uint32_t total;
+        uint32_t ex = carry + block_scan(s, sums, &total) - s;
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            const int64_t i = c0 + (int64_t)threadIdx.x * 4 + j;
+            if (i < len) row[i] = ex;
+            ex += v[j];
+        }
+        carry += total;
+    }
+    if (threadIdx.x == 0) totals[blockIdx.x] = carry;
+}
+
+// PIn: permutation entries read (nullptr: the identity); POut: written.
+template <class K, class PIn, class POut>
+__global__ void __launch_bounds__(kThreads)
+k_sort_downsweep(const K* __restrict__ keys_in, K in_flip, const PIn* __restrict__ perm_in, K* __restrict__ keys_out,
+                 K out_flip, POut* __restrict__ perm_out, int64_t n, int shift, uint32_t mask,
+                 const uint32_t* __restrict__ hist, const uint32_t* __restrict__ totals, int64_t n_tiles) {
+    __shared__ uint32_t base[kBins];
+    __shared__ uint32_t wcnt[2][kWarps][kBins];
+    __shared__ uint32_t sums[kWarps];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    {
+        const uint32_t tot = totals[tid];
+        uint32_t all;
+        const uint32_t start = block_scan(tot, sums, &all) - tot;
+        base[tid] = start + hist[(int64_t)tid * n_tiles + blockIdx.x];
+    }
+    uint32_t run = 0;  // keys of digit tid this tile already placed
+    const int64_t t0 = (int64_t)blockIdx.x * kTile;
+    for (int r = 0; r < kRounds; ++r) {
+        uint32_t(*cnt)[kBins] = wcnt[r & 1];
+        const int64_t i = t0 + (int64_t)r * kThreads + tid;
+        const bool ok = i < n;
+        K k = 0;
+        int d = kBins;  // lanes past the end: a digit no real key has
+        if (ok) {
+            k = keys_in[i] ^ in_flip;
+            d = digit_of<K>(k, shift, mask);
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, d);
+        const uint32_t lrank = (uint32_t)__popc(peers & ((1u << lane) - 1u));
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) cnt[w][tid] = 0u;
+        __syncthreads();
+        if (ok && lrank == 0u) cnt[warp][d] = (uint32_t)__popc(peers);
+        __syncthreads();
+        // the owner of digit tid: exclusive prefix over the warps of this round
+        uint32_t acc = run;
+#pragma unroll
+        for (int w = 0; w < kWarps; ++w) {
+            const uint32_t c = cnt[w][tid];
+            cnt[w][tid] = acc;
+            acc += c;
+        }
+        run = acc;
+        __syncthreads();
+        if (ok) {
+            const uint32_t pos = base[d] + cnt[warp][d] + lrank;
+            if (keys_out) keys_out[pos] = k ^ out_flip;
+            perm_out[pos] = perm_in ? (POut)perm_in[i] : (POut)i;
+        }
+    }
+}
+
+template <class K>
+__global__ void __launch_bounds__(kThreads)
+k_run_count(const K* __restrict__ keys, int64_t n, uint32_t* __restrict__ counts) {
+    __shared__ uint32_t sums[kWarps];
+    const int64_t t0 = (int64_t)blockIdx.x * kTile;
+    uint32_t c = 0;
+    for (int r = 0; r < kRounds; ++r) {
+        const int64_t i = t0 + (int64_t)r * kThreads + threadIdx.x;
+        if (i < n && (i == 0 || keys[i] != keys[i - 1])) ++c;
+    }
+    uint32_t total;
+    block_scan(c, sums, &total);
+    if (threadIdx.x == 0) counts[blockIdx.x] = total;
+}
+
+// starts[j] = position of the j-th run (in key order), starts[runs] = n,
+// *count = runs + 1.  offs: exclusive prefix of the per-tile run counts.
+template <class K, class O>
+__global__ void __launch_bounds__(kThreads)
+k_run_write(const K* __restrict__ keys, int64_t n, const uint32_t* __restrict__ offs,
+            const uint32_t* __restrict__ total, int64_t n_tiles, O* __restrict__ starts, int64_t* __restrict__ count) {
+    __shared__ uint32_t sums[kWarps];
+    const int64_t t0 = (int64_t)blockIdx.x * kTile;
+    uint32_t pos = offs[blockIdx.x];
+    for (int r = 0; r < kRounds; ++r) {
+        const int64_t i = t0 + (int64_t)r * kThreads + threadIdx.x;
+        const uint32_t f = (i < n && (i == 0 || keys[i] != keys[i - 1])) ? 1u : 0u;
+        uint32_t round_total;
+        const uint32_t incl = block_scan(f, sums, &round_total);
+        if (f) starts[pos + incl - 1u] = (O)i;
+        pos += round_total;
+    }
+    if (blockIdx.x == n_tiles - 1 && threadIdx.x == 0) {
+        starts[*total] = (O)n;
+        *count = (int64_t)*total + 1;
+    }
+}
+
+inline int64_t align256(int64_t b) { return (b + 255) & ~(int64_t)255; }
+
+struct SortLayout {
+    int64_t n_tiles = 0, passes = 0, hist = 0, totals = 0, keys_a = 0, perm_a = 0, keys_b = 0, perm_b = 0, bytes = 0;
+};
+
+inline SortLayout sort_layout(int64_t n, int key_size, int key_bits) {
+    SortLayout L;
+    L.n_tiles = ceil_div(n, (int64_t)kTile);
+    L.passes = (key_bits + 7) / 8;
+    int64_t o = 0;
+    L.hist = o;
+    o += align256((int64_t)kBins * L.n_tiles * 4);
+    L.totals = o;
+    o += align256((int64_t)kBins * 4);
+    const int64_t bufs = L.passes - 1 < 2 ? L.passes - 1 : 2;
+    if (bufs >= 1) {
+        L.keys_a = o;
+        o += align256(n * key_size);
+        L.perm_a = o;
+        o += align256(n * 4);
+    }
+    if (bufs >= 2) {
+        L.keys_b = o;
+        o += align256(n * key_size);
+        L.perm_b = o;
+        o += align256(n * 4);
+    }
+    L.bytes = o;
+    return L;
+}
+
+template <class K>
+int run_sort(const K* keys, int64_t n, int key_bits, bool signed_full, K* keys_out, int64_t* order_out, char* ws,
+             const SortLayout& L, cudaStream_t st) {
+    const K flip = signed_full ? (K)((K)1 << (8 * sizeof(K) - 1)) : (K)0;
+    uint32_t* hist = reinterpret_cast<uint32_t*>(ws + L.hist);
+    uint32_t* totals = reinterpret_cast<uint32_t*>(ws + L.totals);
+    K* kb[2] = {reinterpret_cast<K*>(ws + L.keys_a), reinterpret_cast<K*>(ws + L.keys_b)};
+    uint32_t* pb[2] = {reinterpret_cast<uint32_t*>(ws + L.perm_a), reinterpret_cast<uint32_t*>(ws + L.perm_b)};
+    const unsigned grid = (unsigned)L.n_tiles;
+    for (int p = 0; p < L.passes; ++p) {
+        const int shift = 8 * p;
+        const int bits = key_bits - shift < 8 ? key_bits - shift : 8;
+        const uint32_t mask = (1u << bits) - 1u;
+        const bool first = p == 0, last = p == L.passes - 1;
+        const K* kin = first ? keys : kb[(p - 1) & 1];
+        const K fin = first ? flip : (K)0;  // intermediate keys are stored flipped
+        const uint32_t* pin = first ? nullptr : pb[(p - 1) & 1];
+        k_sort_upsweep<K><<<grid, kThreads, 0, st>>>(kin, n, fin, shift, mask, hist, L.n_tiles);
+        k_scan_rows<<<kBins, kThreads, 0, st>>>(hist, L.n_tiles, totals);
+        if (last)
+            k_sort_downsweep<K, uint32_t, int64_t><<<grid, kThreads, 0, st>>>(
+                kin, fin, pin, keys_out, flip, order_out, n, shift, mask, hist, totals, L.n_tiles);
+        else
+            k_sort_downsweep<K, uint32_t, uint32_t><<<grid, kThreads, 0, st>>>(
+                kin, fin, pin, kb[p & 1], (K)0, pb[p & 1], n, shift, mask, hist, totals, L.n_tiles);
+        const int rc = fsb_host::check_launch("k_sort_downsweep");
+        if (rc) return rc;
+    }
+    return FSB_OK;
+}
+
+}  // namespace sort
+}  // namespace fsb
+
+using namespace fsb;
+
+static int sort_args(int64_t n, int key_dtype, int key_bits, const char* who) {
+    if (key_dtype != FSB_I32 && key_dtype != FSB_I64) {
+        fsb_host::set_error("%s: keys must be int32 or int64", who);
+        return FSB_ERR_UNSUPPORTED;
+    }
+    const int width = key_dtype == FSB_I32 ? 32 : 64;
+    if (n < 0 || key_bits < 1 || key_bits > width) {
+        fsb_host::set_error("%s: bad size or key_bits", who);
+        return FSB_ERR_INVALID;
+    }
+    if (n > 0x7fffffffLL) {
+        fsb_host::set_error("%s: %lld keys exceed the 2^31 - 1 limit", who, (long long)n);
+        return FSB_ERR_LIMIT;
+    }
+    return FSB_OK;
+}
+
+extern "C" int64_t fsb_sort_workspace_bytes(int64_t n, int key_dtype, int key_bits) {
+    if (sort_args(n, key_dtype, key_bits, "fsb_sort_workspace_bytes") != FSB_OK) return -1;
+    return sort::sort_layout(n, key_dtype == FSB_I32 ? 4 : 8, key_bits).bytes;
+}
+
+extern "C" int fsb_stable_sort(const void* keys, int key_dtype, int64_t n, int key_bits, void* keys_out,
+                               int64_t* order_out, void* workspace, int64_t workspace_bytes, void* stream) {
+    int rc = sort_args(n, key_dtype, key_bits, "fsb_stable_sort");
+    if (rc) return rc;
+    if (n == 0) return FSB_OK;
+    if (!keys || !order_out) {
+        fsb_host::set_error("fsb_stable_sort: null pointer");
+        return FSB_ERR_INVALID;
+    }
+    const int width = key_dtype == FSB_I32 ? 32 : 64;
+    const sort::SortLayout L = sort::sort_layout(n, width / 8, key_bits);
+    if (!workspace || workspace_bytes < L.bytes) {
+        fsb_host::set_error("fsb_stable_sort: workspace %lld bytes < %lld", (long long)workspace_bytes,
+                            (long long)L.bytes);
+        return FSB_ERR_WORKSPACE;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    char* ws = static_cast<char*>(workspace);
+    const bool signed_full = key_bits == width;
+    if (width == 32)
+        return sort::run_sort<uint32_t>(static_cast<const uint32_t*>(keys), n, key_bits, signed_full,
+                                        static_cast<uint32_t*>(keys_out), order_out, ws, L, st);
+    return sort::run_sort<uint64_t>(static_cast<const uint64_t*>(keys), n, key_bits, signed_full,
+                                    static_cast<uint64_t*>(keys_out), order_out, ws, L, st);
+}
+
+extern "C" int64_t fsb_run_starts_workspace_bytes(int64_t n) {
+    if (n < 0) return -1;
+    return sort::align256(ceil_div(n, (int64_t)sort::kTile) * 4) + 256;
+}
+
+extern "C" int fsb_run_starts(const void* sorted_keys, int key_dtype, int64_t n, void* starts, int starts_dtype,
+                              int64_t* count, void* workspace, int64_t workspace_bytes, void* stream) {
+    int rc = sort_args(n, key_dtype, key_dtype == FSB_I32 ? 32 : 64, "fsb_run_starts");
+    if (rc) return rc;
+    if (starts_dtype != FSB_I32 && starts_dtype != FSB_I64) {
+        fsb_host::set_error("fsb_run_starts: starts must be int32 or int64");
+        return FSB_ERR_UNSUPPORTED;
+    }
+    if (n == 0) return FSB_OK;
+    if (!sorted_keys || !starts || !count) {
+        fsb_host::set_error("fsb_run_starts: null pointer");
+        return FSB_ERR_INVALID;
+    }
+    const int64_t need = fsb_run_starts_workspace_bytes(n);
+    if (!workspace || workspace_bytes < need) {
+        fsb_host::set_error("fsb_run_starts: workspace %lld bytes < %lld", (long long)workspace_bytes,
+                            (long long)need);
+        return FSB_ERR_WORKSPACE;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t n_tiles = ceil_div(n, (int64_t)sort::kTile);
+    uint32_t* counts = static_cast<uint32_t*>(workspace);
+    uint32_t* total = reinterpret_cast<uint32_t*>(static_cast<char*>(workspace) + sort::align256(n_tiles * 4));
+    auto go = [&](auto tk, auto to) -> int {
+        using K = typename decltype(tk)::type;
+        using O = typename decltype(to)::type;
+        const K* keys = static_cast<const K*>(sorted_keys);
+        sort::k_run_count<K><<<(unsigned)n_tiles, sort::kThreads, 0, st>>>(keys, n, counts);
+        sort::k_scan_rows<<<1, sort::kThreads, 0, st>>>(counts, n_tiles, total);
+        sort::k_run_write<K, O><<<(unsigned)n_tiles, sort::kThreads, 0, st>>>(keys, n, counts, total, n_tiles,
+                                                                              static_cast<O*>(starts), count);
+        return fsb_host::check_launch("k_run_write");
+    };
+    if (key_dtype == FSB_I32) {
+        if (starts_dtype == FSB_I32) return go(tag<int32_t>{}, tag<int32_t>{});
+        return go(tag<int32_t>{}, tag<int64_t>{});
+    }
+    if (starts_dtype == FSB_I32) return go(tag<int64_t>{}, tag<int32_t>{});
+    return go(tag<int64_t>{}, tag<int64_t>{});
+}

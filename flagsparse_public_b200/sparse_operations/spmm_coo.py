@@ -35,14 +35,15 @@ def _spmm_coo_compute_dtype(value_dtype):
     return value_dtype
 
 
-def _sort_coo_lex_inplace(data, row, col, n_cols):
+def _sort_coo_lex_inplace(data, row, col, n_cols, n_rows=None):
     """Lexicographic (row, col) order with int64 indices (FlagSparse ``spmm_coo.py:21-32``)."""
     row64 = row.to(torch.int64)
     col64 = col.to(torch.int64)
     if data.numel() == 0:
         return data.contiguous(), row64, col64
     key = row64 * max(1, int(n_cols)) + col64
-    _, order = torch.sort(key, stable=True)
+    bound = None if n_rows is None else max(1, int(n_rows)) * max(1, int(n_cols))
+    _, order = _plan.stable_sort(key, key_bound=bound)
     return data[order].contiguous(), row64[order].contiguous(), col64[order].contiguous()
 
 
@@ -62,9 +63,7 @@ def _seg_starts_from_sorted_rows(row_i32, nnz, device):
     """int32 row-run offsets of sorted COO (FlagSparse ``spmm_coo.py:121-132``)."""
     if nnz == 0:
         return None
-    breaks = torch.nonzero(row_i32[1:] != row_i32[:-1], as_tuple=False).flatten().to(torch.int32) + 1
-    return torch.cat([torch.zeros(1, dtype=torch.int32, device=device), breaks,
-                      torch.tensor([nnz], dtype=torch.int32, device=device)])
+    return _plan.run_starts(row_i32, torch.int32)
 
 
 def _prepare_spmm_coo_inputs(data, row, col, B, shape):
@@ -149,11 +148,9 @@ def _coo_rows_to_csr(data, row, col, n_rows):
     """Order nonzeros by row (stable) and build int64 row offsets."""
     row64 = row.to(torch.int64)
     if data.numel() > 1:
-        sorted_rows, order = torch.sort(row64, stable=True)
+        sorted_rows, order = _plan.stable_sort(row64, key_bound=n_rows)
         data, col, row64 = data[order], col[order], sorted_rows
-    indptr = torch.zeros(n_rows + 1, dtype=torch.int64, device=data.device)
-    if data.numel() > 0:
-        indptr[1:] = torch.cumsum(torch.bincount(row64, minlength=n_rows), 0)
+    indptr = _plan.sorted_keys_to_offsets(row64, n_rows)
     return data.contiguous(), col.contiguous(), indptr
 
 

@@ -117,14 +117,15 @@ class PreparedCoo:
         self._plan = None
 
 
-def _sort_coo_lex_inplace(data, row, col, n_cols):
+def _sort_coo_lex_inplace(data, row, col, n_cols, n_rows=None):
     """Lexicographic (row, col) order; indices promoted to a common dtype
     (FlagSparse ``spmv_coo.py:297-309``)."""
     index_dtype = torch.promote_types(row.dtype, col.dtype)
     if data.numel() == 0:
         return data.contiguous(), row.to(index_dtype).contiguous(), col.to(index_dtype).contiguous()
     key = row.to(torch.int64) * max(1, int(n_cols)) + col.to(torch.int64)
-    _, order = torch.sort(key, stable=True)
+    bound = None if n_rows is None else max(1, int(n_rows)) * max(1, int(n_cols))
+    _, order = _plan.stable_sort(key, key_bound=bound)
     return data[order].contiguous(), row[order].to(index_dtype).contiguous(), col[order].to(index_dtype).contiguous()
 
 
@@ -133,12 +134,7 @@ def _seg_starts_from_sorted_rows(row, nnz, device):
     if nnz == 0:
         return None
     index_dtype = row.dtype if nnz <= _INDEX_LIMIT_INT32 else torch.int64
-    breaks = torch.nonzero(row[1:] != row[:-1], as_tuple=False).flatten().to(index_dtype) + 1
-    return torch.cat([
-        torch.zeros(1, dtype=index_dtype, device=device),
-        breaks,
-        torch.tensor([nnz], dtype=index_dtype, device=device),
-    ])
+    return _plan.run_starts(row, index_dtype)
 
 
 def _prepare_coo_tensors(data, row, col, shape, sort_by_row):
@@ -159,7 +155,7 @@ def _prepare_coo_tensors(data, row, col, shape, sort_by_row):
         raise TypeError("col dtype must be torch.int32 or torch.int64")
     index_dtype = torch.promote_types(row.dtype, col.dtype)
     if sort_by_row:
-        data, kr, kc = _sort_coo_lex_inplace(data, row, col, n_cols)
+        data, kr, kc = _sort_coo_lex_inplace(data, row, col, n_cols, n_rows)
         seg = _seg_starts_from_sorted_rows(kr, data.numel(), data.device)
     else:
         data = data.contiguous()

@@ -208,7 +208,7 @@ def _transpose_csr_for_spmv(data, indices, indptr, shape):
     row_ids = torch.repeat_interleave(torch.arange(n_rows, dtype=torch.int64, device=device), counts,
                                       output_size=nnz)
     cols = indices.to(torch.int64)
-    sorted_cols, order = torch.sort(cols, stable=True)
+    sorted_cols, order = _plan.stable_sort(cols, key_bound=n_cols)
     t_indptr = _plan.sorted_keys_to_offsets(sorted_cols, n_cols)
     return (
         data[order].contiguous(),
@@ -577,7 +577,7 @@ def coo_to_csr_for_spmv(data, row, col, shape, assume_sorted=False):
         row_s, col_s, data_s = row64, col64, data
     else:
         key = row64 * max(1, n_cols) + col64
-        _, order = torch.sort(key, stable=True)
+        _, order = _plan.stable_sort(key, key_bound=max(1, n_rows) * max(1, n_cols))
         row_s, col_s, data_s = row64[order], col64[order], data[order]
     # row offsets on the device, no host read: with assume_sorted the whole
     # conversion can be captured in a CUDA graph

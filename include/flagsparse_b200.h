@@ -208,6 +208,33 @@ int fsb_spmm_coo_atomic(const void* values, const void* row, const void* col,
 int fsb_sorted_keys_to_offsets(const void* keys, int key_dtype, int64_t n,
                                int64_t n_bins, int64_t* offsets, void* stream);
 
+/* ---- integer prepare steps ---------------------------------------------- *
+ * Stable sort of n int32 / int64 keys (key_dtype FSB_I32 / FSB_I64):
+ * keys_out (may be NULL) receives the keys in ascending order and
+ * order_out[n] (int64) the permutation, ties in input order -- the same
+ * result as torch.sort(keys, stable=True).  key_bits < the key width
+ * promises keys in [0, 2^key_bits) (one 8-bit radix pass per started byte);
+ * key_bits = the width sorts any values, signed.  n < 2^31.  Workspace:
+ * fsb_sort_workspace_bytes(n, key_dtype, key_bits) bytes (-1 for bad
+ * arguments).  Replaces the stable argsorts of _transpose_csr_for_spmv
+ * (spmv_csr.py:456-494), coo_to_csr_for_spmv (spmv_csr.py:885-909) and
+ * _sort_coo_lex_inplace (spmv_coo.py:297-309, spmm_coo.py:21-32).         */
+int64_t fsb_sort_workspace_bytes(int64_t n, int key_dtype, int key_bits);
+int fsb_stable_sort(const void* keys, int key_dtype, int64_t n, int key_bits,
+                    void* keys_out, int64_t* order_out, void* workspace,
+                    int64_t workspace_bytes, void* stream);
+
+/* Starts of the runs of equal keys in n sorted int32 / int64 keys: starts
+ * (capacity n + 1, int32 or int64 by starts_dtype) receives 0, the index of
+ * every key that differs from its predecessor, and n; *count (device
+ * int64) the number of entries written.  Replaces the nonzero-based
+ * _seg_starts_from_sorted_rows (spmv_coo.py:312-327, spmm_coo.py:121-132).
+ * Workspace: fsb_run_starts_workspace_bytes(n).                            */
+int64_t fsb_run_starts_workspace_bytes(int64_t n);
+int fsb_run_starts(const void* sorted_keys, int key_dtype, int64_t n,
+                   void* starts, int starts_dtype, int64_t* count,
+                   void* workspace, int64_t workspace_bytes, void* stream);
+
 /* ---- block-sparse SpMM on the tensor cores ----------------------------- *
  * C (float32, n_rows x n_dense, row stride ldc) = A B for A in BSR form with
  * dense 16 x 16 blocks: block_values[n_blocks][16][16] (row-major blocks,
