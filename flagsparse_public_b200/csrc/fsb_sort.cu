@@ -17,10 +17,11 @@
 //     then ranks its keys in rounds of 256 (one per thread, in key order):
 //     __match_any_sync groups the warp's equal digits, per-warp digit counts
 //     in shared memory are prefixed over the warps by the thread that owns
-//     the digit, and the key and its permutation entry are written to
-//     digit start + tile prefix + rank.  Ranks follow key order inside the
-//     tile and tiles follow each other, so every pass is stable and the
-//     result equals a stable sort (torch.sort(stable=True)) bit for bit.
+//     the digit; the tile is staged in shared memory in digit order and
+//     written out in order, key and permutation entry to digit start + tile
+//     prefix + rank.  Ranks follow key order inside the tile and tiles
+//     follow each other, so every pass is stable and the result equals a
+//     stable sort (torch.sort(stable=True)) bit for bit.
 // The permutation travels as 32-bit indices between passes and is written as
 // int64 by the last pass.  Keys of the full signed width are ordered through
 // their top bit flipped.  HBM bound: a pass reads the keys twice and the
@@ -117,33 +118,50 @@ k_scan_rows(uint32_t* __restrict__ rows, int64_t len, uint32_t* __restrict__ tot
 }
 
 // PIn: permutation entries read (nullptr: the identity); POut: written.
+// The tile's keys are ranked in registers (rank among the tile's keys of
+// the same digit), staged in shared memory in digit order, and written from
+// there in order, so each digit's run of the tile leaves as consecutive
+// stores.
 template <class K, class PIn, class POut>
 __global__ void __launch_bounds__(kThreads)
 k_sort_downsweep(const K* __restrict__ keys_in, K in_flip, const PIn* __restrict__ perm_in, K* __restrict__ keys_out,
                  K out_flip, POut* __restrict__ perm_out, int64_t n, int shift, uint32_t mask,
                  const uint32_t* __restrict__ hist, const uint32_t* __restrict__ totals, int64_t n_tiles) {
-    __shared__ uint32_t base[kBins];
+    __shared__ uint32_t gbase[kBins];  // output position of the tile's first key of each digit
+    __shared__ uint32_t lbase[kBins];  // its position in the staged tile
     __shared__ uint32_t wcnt[2][kWarps][kBins];
     __shared__ uint32_t sums[kWarps];
+    extern __shared__ __align__(16) unsigned char staged[];  // downsweep_smem<K>() bytes
+    K* skey = reinterpret_cast<K*>(staged);
+    uint32_t* sidx = reinterpret_cast<uint32_t*>(staged + kTile * sizeof(K));
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int64_t t0 = (int64_t)blockIdx.x * kTile;
+    const int n_here = (int)((n - t0) < kTile ? (n - t0) : kTile);
+    K k[kRounds];
+    uint32_t src[kRounds];
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+        const int64_t i = t0 + (int64_t)r * kThreads + tid;
+        k[r] = 0;
+        src[r] = 0;
+        if (i < n) {
+            k[r] = keys_in[i] ^ in_flip;
+            src[r] = perm_in ? (uint32_t)perm_in[i] : (uint32_t)i;
+        }
+    }
     {
         const uint32_t tot = totals[tid];
         uint32_t all;
         const uint32_t start = block_scan(tot, sums, &all) - tot;
-        base[tid] = start + hist[(int64_t)tid * n_tiles + blockIdx.x];
+        gbase[tid] = start + hist[(int64_t)tid * n_tiles + blockIdx.x];
     }
-    uint32_t run = 0;  // keys of digit tid this tile already placed
-    const int64_t t0 = (int64_t)blockIdx.x * kTile;
+    uint32_t run = 0;  // keys of digit tid ranked so far in this tile
+    uint32_t rank[kRounds];
+#pragma unroll
     for (int r = 0; r < kRounds; ++r) {
         uint32_t(*cnt)[kBins] = wcnt[r & 1];
-        const int64_t i = t0 + (int64_t)r * kThreads + tid;
-        const bool ok = i < n;
-        K k = 0;
-        int d = kBins;  // lanes past the end: a digit no real key has
-        if (ok) {
-            k = keys_in[i] ^ in_flip;
-            d = digit_of<K>(k, shift, mask);
-        }
+        const bool ok = r * kThreads + tid < n_here;
+        const int d = ok ? digit_of<K>(k[r], shift, mask) : kBins;  // lanes past the end: no real digit
         const unsigned peers = __match_any_sync(0xffffffffu, d);
         const uint32_t lrank = (uint32_t)__popc(peers & ((1u << lane) - 1u));
 #pragma unroll
@@ -161,11 +179,28 @@ k_sort_downsweep(const K* __restrict__ keys_in, K in_flip, const PIn* __restrict
         }
         run = acc;
         __syncthreads();
-        if (ok) {
-            const uint32_t pos = base[d] + cnt[warp][d] + lrank;
-            if (keys_out) keys_out[pos] = k ^ out_flip;
-            perm_out[pos] = perm_in ? (POut)perm_in[i] : (POut)i;
+        rank[r] = ok ? cnt[warp][d] + lrank : 0u;
+    }
+    {
+        uint32_t all;
+        lbase[tid] = block_scan(run, sums, &all) - run;  // digit starts inside the tile
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < kRounds; ++r) {
+        if (r * kThreads + tid < n_here) {
+            const uint32_t p = lbase[digit_of<K>(k[r], shift, mask)] + rank[r];
+            skey[p] = k[r];
+            sidx[p] = src[r];
         }
+    }
+    __syncthreads();
+    for (int j = tid; j < n_here; j += kThreads) {
+        const K kk = skey[j];
+        const int d = digit_of<K>(kk, shift, mask);
+        const uint32_t pos = gbase[d] + ((uint32_t)j - lbase[d]);
+        if (keys_out) keys_out[pos] = kk ^ out_flip;
+        perm_out[pos] = (POut)sidx[j];
     }
 }
 
@@ -205,6 +240,12 @@ k_run_write(const K* __restrict__ keys, int64_t n, const uint32_t* __restrict__ 
         starts[*total] = (O)n;
         *count = (int64_t)*total + 1;
     }
+}
+
+// Dynamic shared memory of k_sort_downsweep: the staged keys and permutation.
+template <class K>
+constexpr int downsweep_smem() {
+    return kTile * ((int)sizeof(K) + 4);
 }
 
 inline int64_t align256(int64_t b) { return (b + 255) & ~(int64_t)255; }
@@ -258,12 +299,24 @@ int run_sort(const K* keys, int64_t n, int key_bits, bool signed_full, K* keys_o
         const uint32_t* pin = first ? nullptr : pb[(p - 1) & 1];
         k_sort_upsweep<K><<<grid, kThreads, 0, st>>>(kin, n, fin, shift, mask, hist, L.n_tiles);
         k_scan_rows<<<kBins, kThreads, 0, st>>>(hist, L.n_tiles, totals);
-        if (last)
-            k_sort_downsweep<K, uint32_t, int64_t><<<grid, kThreads, 0, st>>>(
-                kin, fin, pin, keys_out, flip, order_out, n, shift, mask, hist, totals, L.n_tiles);
-        else
-            k_sort_downsweep<K, uint32_t, uint32_t><<<grid, kThreads, 0, st>>>(
-                kin, fin, pin, kb[p & 1], (K)0, pb[p & 1], n, shift, mask, hist, totals, L.n_tiles);
+        constexpr int dyn = downsweep_smem<K>();
+        if (last) {
+            auto kern = k_sort_downsweep<K, uint32_t, int64_t>;
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess) {
+                fsb_host::set_error("fsb_stable_sort: cannot reserve %d bytes of shared memory", dyn);
+                return FSB_ERR_LAUNCH;
+            }
+            kern<<<grid, kThreads, dyn, st>>>(kin, fin, pin, keys_out, flip, order_out, n, shift, mask, hist, totals,
+                                              L.n_tiles);
+        } else {
+            auto kern = k_sort_downsweep<K, uint32_t, uint32_t>;
+            if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, dyn) != cudaSuccess) {
+                fsb_host::set_error("fsb_stable_sort: cannot reserve %d bytes of shared memory", dyn);
+                return FSB_ERR_LAUNCH;
+            }
+            kern<<<grid, kThreads, dyn, st>>>(kin, fin, pin, kb[p & 1], (K)0, pb[p & 1], n, shift, mask, hist,
+                                              totals, L.n_tiles);
+        }
         const int rc = fsb_host::check_launch("k_sort_downsweep");
         if (rc) return rc;
     }
