@@ -13,6 +13,8 @@ float16/bfloat16 in float32 (``:544-551``) -- in registers, with no widened
 copies of A and B; the opt path accumulates in the value precision (``:631``).
 """
 
+import math
+
 from ._common import *
 from ._common import _device_checks
 from .. import _native as _nat
@@ -97,10 +99,11 @@ def _spmm_validation_metrics(candidate, reference):
     return metrics
 
 
-def _prepare_spmm_csr_matrix(data, indices, indptr, shape):
+def _prepare_spmm_csr_matrix(data, indices, indptr, shape, return_stats=False):
     """Validation of FlagSparse ``spmm_csr.py:197-255`` with one device->host
     read for all structural checks.  Returns int32 column indices (int64 ones
-    converted, as the reference does) and int64 indptr."""
+    converted, as the reference does) and int64 indptr; with ``return_stats``
+    also the row-length statistics of the plan heuristics, from the same read."""
     if len(shape) != 2:
         raise ValueError("shape must be a 2-tuple: (n_rows, n_cols)")
     if data.ndim != 1 or indices.ndim != 1 or indptr.ndim != 1:
@@ -130,6 +133,9 @@ def _prepare_spmm_csr_matrix(data, indices, indptr, shape):
     if nnz > 0:
         checks += [indices.min(), indices.max()]
     checks.append(row_lengths.max() if n_rows > 0 else zero)
+    if return_stats:
+        checks += [(row_lengths * row_lengths).sum() if n_rows > 0 else zero,
+                   (row_lengths == 0).sum() if n_rows > 0 else zero]
     vals = _device_checks(checks)
     if indptr.numel() > 0 and int(vals[0]) != 0:
         raise ValueError("indptr[0] must be 0")
@@ -149,8 +155,19 @@ def _prepare_spmm_csr_matrix(data, indices, indptr, shape):
     indptr = indptr.contiguous()
     kernel_indices = indices.to(torch.int32) if indices.dtype == torch.int64 else indices
     kernel_indptr = indptr.to(torch.int64)
+    if return_stats:
+        sum_sq, empty = vals[-2], vals[-1]
+        vals = vals[:-2]
     max_row_nnz = int(vals[-1]) if n_rows > 0 else 0
-    return data, kernel_indices, kernel_indptr, n_rows, n_cols, row_lengths, max_row_nnz
+    if not return_stats:
+        return data, kernel_indices, kernel_indptr, n_rows, n_cols, row_lengths, max_row_nnz
+    if n_rows == 0:
+        stats = _plan.MatrixStats(0, n_cols, 0, 0, 0.0, 0.0, 0)
+    else:
+        mean = nnz / n_rows
+        std = math.sqrt(max(sum_sq / n_rows - mean * mean, 0.0))
+        stats = _plan.MatrixStats(n_rows, n_cols, nnz, max_row_nnz, mean, std, empty)
+    return data, kernel_indices, kernel_indptr, n_rows, n_cols, row_lengths, max_row_nnz, stats
 
 
 def _prepare_spmm_csr_inputs(data, indices, indptr, B, shape):
@@ -232,14 +249,9 @@ class PreparedCsrSpmmOpt:
         "n_cols",
         "row_lengths",
         "max_row_nnz",
-        "row_buckets",
         "supports_opt",
-        "long_part_rows",
-        "long_part_starts",
-        "long_part_ends",
-        "long_row_ids",
-        "long_row_part_ptr",
         "long_row_fallback_only",
+        "_bucket_meta",
         "_stats",
         "_plans",
     )
@@ -254,13 +266,13 @@ class PreparedCsrSpmmOpt:
         n_cols,
         row_lengths,
         max_row_nnz,
-        row_buckets,
-        long_part_rows,
-        long_part_starts,
-        long_part_ends,
-        long_row_ids,
-        long_row_part_ptr,
-        long_row_fallback_only,
+        row_buckets=None,
+        long_part_rows=None,
+        long_part_starts=None,
+        long_part_ends=None,
+        long_row_ids=None,
+        long_row_part_ptr=None,
+        long_row_fallback_only=False,
     ):
         self.data = data
         self.kernel_indices = kernel_indices
@@ -270,16 +282,48 @@ class PreparedCsrSpmmOpt:
         self.n_cols = int(n_cols)
         self.row_lengths = row_lengths
         self.max_row_nnz = int(max_row_nnz)
-        self.row_buckets = row_buckets
         self.supports_opt = data.dtype in (torch.float32, torch.float64)
-        self.long_part_rows = long_part_rows
-        self.long_part_starts = long_part_starts
-        self.long_part_ends = long_part_ends
-        self.long_row_ids = long_row_ids
-        self.long_row_part_ptr = long_row_part_ptr
+        given = (row_buckets, long_part_rows, long_part_starts, long_part_ends, long_row_ids, long_row_part_ptr)
+        # FlagSparse's bucket lists and long-row split parts describe its own
+        # launches; the kernels here never read them, so a prepare that does
+        # not pass them builds them on first access only
+        self._bucket_meta = None if all(v is None for v in given) else dict(zip(_SPMM_OPT_META_FIELDS, given))
         self.long_row_fallback_only = bool(long_row_fallback_only)
         self._stats = None
         self._plans = {}
+
+    def _meta(self):
+        if self._bucket_meta is None:
+            row_buckets, long_rows = _build_spmm_opt_buckets(self.row_lengths)
+            split = _build_spmm_opt_split_metadata(
+                self.kernel_indptr, long_rows, part_block_nnz=_SPMM_OPT_PART_NNZ
+            ) if long_rows.numel() > 0 else (
+                torch.empty((0,), dtype=long_rows.dtype, device=self.data.device),
+                torch.empty((0,), dtype=torch.int64, device=self.data.device),
+                torch.empty((0,), dtype=torch.int64, device=self.data.device),
+                torch.zeros(1, dtype=torch.int64, device=self.data.device),
+            )
+            self._bucket_meta = dict(zip(_SPMM_OPT_META_FIELDS, (row_buckets, split[0], split[1], split[2],
+                                                                 long_rows, split[3])))
+        return self._bucket_meta
+
+
+_SPMM_OPT_META_FIELDS = ("row_buckets", "long_part_rows", "long_part_starts", "long_part_ends", "long_row_ids",
+                         "long_row_part_ptr")
+
+
+def _meta_property(name):
+    def get(self):
+        return self._meta()[name]
+
+    def set_(self, value):
+        self._meta()[name] = value
+
+    return property(get, set_)
+
+
+for _name in _SPMM_OPT_META_FIELDS:
+    setattr(PreparedCsrSpmmOpt, _name, _meta_property(_name))
 
 
 _SPMM_OPT_LONG_ROW_THRESHOLD = 2048
@@ -338,19 +382,11 @@ def _build_spmm_opt_buckets(row_lengths):
 
 
 def prepare_spmm_csr_opt(data, indices, indptr, shape):
-    (data, kernel_indices, kernel_indptr, n_rows, n_cols, row_lengths, max_row_nnz) = _prepare_spmm_csr_matrix(
-        data, indices, indptr, shape
-    )
-    row_buckets, long_rows = _build_spmm_opt_buckets(row_lengths)
-    long_part_rows, long_part_starts, long_part_ends, long_row_part_ptr = _build_spmm_opt_split_metadata(
-        kernel_indptr, long_rows, part_block_nnz=_SPMM_OPT_PART_NNZ
-    ) if long_rows.numel() > 0 else (
-        torch.empty((0,), dtype=long_rows.dtype, device=data.device),
-        torch.empty((0,), dtype=torch.int64, device=data.device),
-        torch.empty((0,), dtype=torch.int64, device=data.device),
-        torch.zeros(1, dtype=torch.int64, device=data.device),
-    )
-    return PreparedCsrSpmmOpt(
+    """Validated CSR + cached plans; the bucket / split metadata fields
+    (FlagSparse ``spmm_csr.py:480-522``) are built on first access."""
+    (data, kernel_indices, kernel_indptr, n_rows, n_cols, row_lengths, max_row_nnz,
+     stats) = _prepare_spmm_csr_matrix(data, indices, indptr, shape, return_stats=True)
+    p = PreparedCsrSpmmOpt(
         data=data,
         kernel_indices=kernel_indices,
         kernel_indptr=kernel_indptr,
@@ -359,14 +395,10 @@ def prepare_spmm_csr_opt(data, indices, indptr, shape):
         n_cols=n_cols,
         row_lengths=row_lengths,
         max_row_nnz=max_row_nnz,
-        row_buckets=row_buckets,
-        long_part_rows=long_part_rows,
-        long_part_starts=long_part_starts,
-        long_part_ends=long_part_ends,
-        long_row_ids=long_rows,
-        long_row_part_ptr=long_row_part_ptr,
         long_row_fallback_only=False,
     )
+    p._stats = stats
+    return p
 
 
 def _spmm_plan_for(holder, kind, n_dense, operands=None):
