@@ -24,14 +24,16 @@
 //     slice as two 64-column x 16-row boxes of a 2-D tensor map over B
 //     (128-byte swizzle; SWIZZLE_128B MN-major operand) and each block as one
 //     box of a 5-D tensor map over the block array that lands in the K-major
-//     core-matrix order, into a 4-stage ring; one thread runs the pipeline
-//     (loads three blocks ahead, MMA, commit, refill) with no CTA barrier per
-//     block;
+//     core-matrix order, into a 4-stage ring.  Persistent and warp
+//     specialised: one lane loads and issues MMAs across the CTA's block rows,
+//     two TMEM accumulators alternate between rows, four epilogue warps drain
+//     one row while the next accumulates;
 //   * k_bsr_spmm_tc: the CTA's threads copy the slice with 16-byte loads into
 //     two alternating stages (SWIZZLE_NONE MN-major operand).
 //
-// TMEM: 32 columns per CTA; at most 16 CTAs of 128 threads are resident per
-// SM, so allocations never exceed the SM's 512 columns and never wait.
+// TMEM: 32 columns per CTA (two 16-column accumulators in the persistent
+// kernel); at most 16 CTAs are resident per SM, so allocations never exceed
+// the SM's 512 columns and never wait.
 // Every mbarrier wait is bounded (1 s, globaltimer); on expiry the kernel
 // records FSB_ERR_TIMEOUT in the device error word (fsb_device_error), waits
 // (bounded) for the MMA it issued, frees its TMEM and returns.
@@ -216,7 +218,7 @@ k_bsr_spmm_tc(const V* __restrict__ blocks, const I* __restrict__ bcol, const P*
     }
 }
 
-constexpr int kTmaStages = 3;
+constexpr int kTmaStages = 4;
 constexpr int kTmaBoxCols = 64;                      // 128 bytes of 16-bit values
 constexpr int kTmaBoxBytes = kTmaBoxCols * 16 * 2;  // 2 KB per box, 2 boxes per slice
 
@@ -243,49 +245,67 @@ __device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-// One thread runs the pipeline: TMA loads of the B slice (two 64 x 16 boxes
-// of bmap) and of the 16 x 16 block (one box of amap, a 5-D view of the
-// block array whose box lands in the K-major core-matrix order) into a
-// 4-stage ring, the MMA once a stage is full, its commit to the stage's
-// empty barrier, and the refill of the stage three blocks ahead.  No CTA
-// barrier per block: the other warps wait for the last commit only.
+// Persistent, warp-specialised pipeline.  Each CTA takes block rows
+// blockIdx.x, blockIdx.x + gridDim.x, ... of one 128-column tile:
+//   * warp 4, one lane: TMA loads of each stored block's B slice (two 64 x 16
+//     boxes of bmap) and of the 16 x 16 block itself (one box of amap, a 5-D
+//     view of the block array whose box lands in the K-major core-matrix
+//     order) into an S-stage ring, up to S blocks ahead and across block-row
+//     boundaries; the MMA once a stage is full and its commit to the stage's
+//     empty barrier; after a row's last MMA a commit to the row's
+//     accumulator barrier.  Rows alternate between two 16-column TMEM
+//     accumulators, so the next row's MMAs run while the previous row drains;
+//   * warps 0-3 (the four TMEM lane quarters): wait for a row's accumulator,
+//     read it (tcgen05.ld 32x32b, two 8-column halves), release it through
+//     the accumulator-empty barrier and store the 16 C rows.
+// Every wait is bounded; on expiry the waiting thread records
+// FSB_ERR_TIMEOUT, raises the CTA's fail flag (the other roles stop at their
+// next wait), and the MMA lane waits (bounded) for its copies and MMAs in
+// flight before the CTA frees its TMEM.
+constexpr int kPersistWarps = 5;
+constexpr int kPersistThreads = 32 * kPersistWarps;
+constexpr int kPersistCtasPerSm = 8;
+
+// Bounded wait that also gives up when another role raised the fail flag.
+__device__ __forceinline__ bool mbar_wait_or_fail(uint32_t bar, uint32_t parity, volatile int* fail) {
+    if (tma::mbar_test(bar, parity)) return true;
+    const unsigned long long t0 = tma::now_ns();
+    while (!tma::mbar_test(bar, parity)) {
+        if (*fail) return false;
+        if (tma::now_ns() - t0 > tma::kWaitNs) return false;
+    }
+    return true;
+}
+
 template <class V, class I, class P>
-__global__ void __launch_bounds__(kThreads, 16)
+__global__ void __launch_bounds__(kPersistThreads)
 k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const __grid_constant__ CUtensorMap amap,
-               const I* __restrict__ bcol, const P* __restrict__ bptr, int64_t n_rows, int64_t n_dense,
-               float* __restrict__ C, int64_t ldc, int* __restrict__ err) {
+               const I* __restrict__ bcol, const P* __restrict__ bptr, int64_t n_rows, int64_t n_block_rows,
+               int64_t n_dense, float* __restrict__ C, int64_t ldc, int* __restrict__ err) {
     constexpr bool kBf16 = std::is_same<V, __nv_bfloat16>::value;
     constexpr int S = kTmaStages;
     constexpr uint32_t kStageTx = 2 * kTmaBoxBytes + kBStageBytes;
     __shared__ __align__(1024) unsigned char sa[S][2 * kTmaBoxBytes];
     __shared__ __align__(128) unsigned char sb[S][kBStageBytes];
-    __shared__ __align__(8) uint64_t full[S], empty[S];
+    __shared__ __align__(8) uint64_t full[S], empty[S], acc_full[2], acc_empty[2];
     __shared__ uint32_t tmem_base_slot;
-    __shared__ int fail_flag;
+    __shared__ volatile int fail;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int64_t r = blockIdx.x;
     const int64_t c0 = (int64_t)blockIdx.y * kM;
     const int cols = (int)((n_dense - c0) < kM ? (n_dense - c0) : kM);
-    const int64_t b0 = idx(bptr[r]), b1 = idx(bptr[r + 1]);
-    const int nb = (int)(b1 - b0);
-
-    auto issue = [&](int b) {  // thread 0: block b's operands into stage b % S
-        const int s = b % S;
-        const uint32_t bar = smem_u32(&full[s]);
-        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(kStageTx) : "memory");
-        const int y = (int)(idx(bcol[b0 + b]) * 16);
-        tma_load_2d(smem_u32(&sa[s][0]), &bmap, (int)c0, y, bar);
-        tma_load_2d(smem_u32(&sa[s][kTmaBoxBytes]), &bmap, (int)c0 + kTmaBoxCols, y, bar);
-        tma_load_5d(smem_u32(&sb[s][0]), &amap, (int)(b0 + b), bar);
-    };
+    const int64_t stride = gridDim.x;
 
     if (tid == 0) {
         for (int i = 0; i < S; ++i) {
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[i])) : "memory");
-            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[i])) : "memory");
+            tma::mbar_init(smem_u32(&full[i]), 1);
+            tma::mbar_init(smem_u32(&empty[i]), 1);
         }
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        fail_flag = 0;
+        for (int i = 0; i < 2; ++i) {
+            tma::mbar_init(smem_u32(&acc_full[i]), 1);
+            tma::mbar_init(smem_u32(&acc_empty[i]), 4);  // one arrival per epilogue warp
+        }
+        tma::mbar_init_fence();
+        fail = 0;
     }
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
@@ -300,79 +320,133 @@ k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const __grid_constant__
     const uint32_t tmem = tmem_base_slot;
     constexpr uint32_t idesc = instr_desc<kBf16>();
 
-    if (tid == 0) {
-        int issued = 0;
-        for (; issued < nb && issued < S; ++issued) issue(issued);
-        for (int b = 0; b < nb; ++b) {
-            const int s = b % S;
-            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((b / S) & 1))) {
-                fail_flag = 1;
+    if (warp == 4) {
+        if (lane == 0) {
+            // issue cursor: block ib of row ir (ie = the row's end), issued blocks so far
+            int64_t ir = blockIdx.x, ib = 0, ie = 0;
+            if (ir < n_block_rows) {
+                ib = idx(bptr[ir]);
+                ie = idx(bptr[ir + 1]);
+            }
+            uint32_t issued = 0, g = 0;
+            bool ok = true;
+            auto issue_more = [&](uint32_t upto) {  // blocks [issued, upto] of this CTA, as far as they exist
+                while (ok && issued <= upto) {
+                    while (ib >= ie && ir < n_block_rows) {
+                        ir += stride;
+                        if (ir < n_block_rows) {
+                            ib = idx(bptr[ir]);
+                            ie = idx(bptr[ir + 1]);
+                        }
+                    }
+                    if (ir >= n_block_rows) return;
+                    const uint32_t s = issued % S;
+                    if (issued >= (uint32_t)S && !mbar_wait_or_fail(smem_u32(&empty[s]), ((issued / S) - 1) & 1u, &fail)) {
+                        ok = false;
+                        return;
+                    }
+                    const uint32_t bar = smem_u32(&full[s]);
+                    tma::mbar_arrive_expect_tx(bar, kStageTx);
+                    const int y = (int)(idx(bcol[ib]) * 16);
+                    tma_load_2d(smem_u32(&sa[s][0]), &bmap, (int)c0, y, bar);
+                    tma_load_2d(smem_u32(&sa[s][kTmaBoxBytes]), &bmap, (int)c0 + kTmaBoxCols, y, bar);
+                    tma_load_5d(smem_u32(&sb[s][0]), &amap, (int)ib, bar);
+                    ++issued;
+                    ++ib;
+                }
+            };
+            int64_t k = 0;
+            for (int64_t r = blockIdx.x; ok && r < n_block_rows; r += stride, ++k) {
+                const int nb = (int)(idx(bptr[r + 1]) - idx(bptr[r]));
+                const uint32_t buf = (uint32_t)(k & 1);
+                if (k >= 2 && !mbar_wait_or_fail(smem_u32(&acc_empty[buf]), (uint32_t)(((k >> 1) - 1) & 1), &fail)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                for (int j = 0; j < nb; ++j) {
+                    issue_more(g + S - 1);
+                    if (!ok || !mbar_wait_or_fail(smem_u32(&full[g % S]), (g / S) & 1u, &fail)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t s = g % S;
+                    // A: two 64-column groups 2 KB apart (LBO), 8-row groups 1 KB apart (SBO)
+                    const uint64_t adesc = smem_desc_sw128(smem_u32(&sa[s][0]), kTmaBoxBytes, 1024);
+                    const uint64_t bdesc = smem_desc(smem_u32(&sb[s][0]), 128, 256);
+                    const uint32_t accumulate = j > 0 ? 1u : 0u;
+                    const uint32_t zero = 0;
+                    asm volatile(
+                        "{\n\t.reg .pred p;\n\t"
+                        "setp.ne.b32 p, %4, 0;\n\t"
+                        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(
+                            tmem + buf * 16u),
+                        "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(zero), "r"(zero), "r"(zero), "r"(zero)
+                        : "memory");
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                     smem_u32(&empty[s]))
+                                 : "memory");
+                    ++g;
+                }
+                if (!ok) break;
+                // the row's accumulator is final once every MMA issued so far completed
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                                 smem_u32(&acc_full[buf]))
+                             : "memory");
+            }
+            if (!ok) {
+                fail = 1;
+                atomicExch(err, FSB_ERR_TIMEOUT);
+                // drain (bounded): the copies issued and the MMAs committed
+                for (uint32_t q = g; q < issued; ++q) tma::mbar_wait(smem_u32(&full[q % S]), (q / S) & 1u);
+                if (g > 0) tma::mbar_wait(smem_u32(&empty[(g - 1) % S]), ((g - 1) / S) & 1u);
+            }
+        }
+        __syncwarp();
+    } else {
+        // epilogue warps: TMEM lane quarter `warp` = dense columns c0 + 32 warp + lane
+        int64_t k = 0;
+        for (int64_t r = blockIdx.x; r < n_block_rows; r += stride, ++k) {
+            const uint32_t buf = (uint32_t)(k & 1);
+            // warp-uniform outcome: the TMEM loads below are warp-collective
+            const bool ready = __all_sync(0xffffffffu, mbar_wait_or_fail(smem_u32(&acc_full[buf]),
+                                                                         (uint32_t)((k >> 1) & 1), &fail));
+            if (!ready) {
+                if (lane == 0) atomicExch(err, FSB_ERR_TIMEOUT);
+                fail = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // A: two 64-column groups 2 KB apart (LBO), 8-row groups 1 KB apart (SBO)
-            const uint64_t adesc = smem_desc_sw128(smem_u32(&sa[s][0]), kTmaBoxBytes, 1024);
-            const uint64_t bdesc = smem_desc(smem_u32(&sb[s][0]), 128, 256);
-            const uint32_t accumulate = b > 0 ? 1u : 0u;
-            const uint32_t zero = 0;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "setp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n" ::"r"(tmem),
-                "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate), "r"(zero), "r"(zero), "r"(zero), "r"(zero)
-                : "memory");
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
-                             smem_u32(&empty[s]))
-                         : "memory");
-            if (b + S < nb) {
-                if (!mbar_wait(smem_u32(&empty[s]), (uint32_t)((b / S) & 1))) {
-                    fail_flag = 1;
-                    break;
-                }
-                issue(b + S);
-                ++issued;
-            }
-        }
-        if (fail_flag) {
-            // drain (bounded) what is still in flight before TMEM and the ring go away
-            for (int b = issued > S ? issued - S : 0; b < issued; ++b) {
-                mbar_wait(smem_u32(&full[b % S]), (uint32_t)((b / S) & 1));
-                mbar_wait(smem_u32(&empty[b % S]), (uint32_t)((b / S) & 1));
-            }
-        }
-    }
-    // everyone: the last MMA's commit (all earlier MMAs complete before it)
-    bool ok = true;
-    if (nb > 0) {
-        const int last = nb - 1;
-        ok = mbar_wait(smem_u32(&empty[last % S]), (uint32_t)((last / S) & 1));
-    }
-    const bool failed = __syncthreads_or(!ok || fail_flag) != 0;
-    if (failed) {
-        if (tid == 0) atomicExch(err, FSB_ERR_TIMEOUT);
-    } else {
-        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        // two 8-column halves keep the read-out at 8 registers
-        const int m = warp * 32 + lane;
-#pragma unroll
-        for (int h = 0; h < 2; ++h) {
-            uint32_t d[8];
-            if (nb > 0) {
-                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(h * 8);
+            const bool any = idx(bptr[r + 1]) > idx(bptr[r]);
+            uint32_t d[16];
+            if (any) {
+                const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + buf * 16u;
                 asm volatile(
                     "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                     : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7])
                     : "r"(taddr)
                     : "memory");
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                    : "=r"(d[8]), "=r"(d[9]), "=r"(d[10]), "=r"(d[11]), "=r"(d[12]), "=r"(d[13]), "=r"(d[14]),
+                      "=r"(d[15])
+                    : "r"(taddr + 8u)
+                    : "memory");
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             } else {
 #pragma unroll
-                for (int n = 0; n < 8; ++n) d[n] = 0u;
+                for (int n = 0; n < 16; ++n) d[n] = 0u;  // empty block row: zeros
             }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[buf])) : "memory");
+            const int m = warp * 32 + lane;
             if (m < cols) {
 #pragma unroll
-                for (int n = 0; n < 8; ++n) {
-                    const int64_t row = r * 16 + h * 8 + n;
+                for (int n = 0; n < 16; ++n) {
+                    const int64_t row = r * 16 + n;
                     if (row < n_rows) __stcs(C + row * ldc + c0 + m, __uint_as_float(d[n]));
                 }
             }
@@ -477,14 +551,20 @@ extern "C" int fsb_bsr_spmm_tc(const void* block_values, int value_dtype, const 
             using I = typename decltype(ti)::type;
             return fsb::dispatch_idx(ptr_dtype, [&](auto tp) -> int {
                 using P = typename decltype(tp)::type;
+                // persistent grid: kPersistCtasPerSm CTAs per SM and column tile
+                int dev = 0, sms = 148;
+                if (cudaGetDevice(&dev) == cudaSuccess)
+                    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+                const int64_t cap = (int64_t)sms * fsb::bsr::kPersistCtasPerSm;
+                dim3 gp((unsigned)(n_block_rows < cap ? n_block_rows : cap), (unsigned)tiles);
                 if (value_dtype == FSB_BF16)
-                    fsb::bsr::k_bsr_spmm_tma<__nv_bfloat16, I, P><<<g, fsb::bsr::kThreads, 0, st>>>(
+                    fsb::bsr::k_bsr_spmm_tma<__nv_bfloat16, I, P><<<gp, fsb::bsr::kPersistThreads, 0, st>>>(
                         bmap, amap, static_cast<const I*>(block_col), static_cast<const P*>(block_row_ptr), n_rows,
-                        n_dense, C, ldc, err);
+                        n_block_rows, n_dense, C, ldc, err);
                 else
-                    fsb::bsr::k_bsr_spmm_tma<__half, I, P><<<g, fsb::bsr::kThreads, 0, st>>>(
+                    fsb::bsr::k_bsr_spmm_tma<__half, I, P><<<gp, fsb::bsr::kPersistThreads, 0, st>>>(
                         bmap, amap, static_cast<const I*>(block_col), static_cast<const P*>(block_row_ptr), n_rows,
-                        n_dense, C, ldc, err);
+                        n_block_rows, n_dense, C, ldc, err);
                 return fsb_host::check_launch("k_bsr_spmm_tma");
             });
         });
