@@ -40,6 +40,9 @@ _DTYPE_CODES = {
     torch.int32: FSB_I32,
     torch.int64: FSB_I64,
 }
+FSB_C32 = 8
+if getattr(torch, "complex32", None) is not None:
+    _DTYPE_CODES[torch.complex32] = FSB_C32
 
 
 class FsbCsr(ctypes.Structure):

@@ -18,6 +18,7 @@ namespace fsb {
 constexpr int32_t kMaxItemsPerUnit = 1 << 24;
 
 // ---------------------------------------------------------------- types ----
+struct __align__(4) c32_t { __half re, im; };
 struct __align__(8) c64_t { float re, im; };
 struct __align__(16) c128_t { double re, im; };
 
@@ -137,6 +138,20 @@ template <> struct Acc<c64_t, c64_t> {
         return acc;
     }
 };
+// complex32: float16 pairs widened to float32 in registers (FlagSparse
+// accumulates complex32 in float32, spmm_csr.py:576-598)
+template <> struct Acc<c32_t, c64_t> {
+    static __device__ __forceinline__ c64_t zero() { return c64_t{0.f, 0.f}; }
+    static __device__ __forceinline__ c64_t fma(c32_t a, c32_t b, c64_t acc) {
+        const float ar = __half2float(a.re), ai = __half2float(a.im);
+        const float br = __half2float(b.re), bi = __half2float(b.im);
+        acc.re = fmaf(ar, br, acc.re);
+        acc.re = fmaf(-ai, bi, acc.re);
+        acc.im = fmaf(ar, bi, acc.im);
+        acc.im = fmaf(ai, br, acc.im);
+        return acc;
+    }
+};
 template <> struct Acc<c64_t, c128_t> {
     static __device__ __forceinline__ c128_t zero() { return c128_t{0.0, 0.0}; }
     static __device__ __forceinline__ c128_t fma(c64_t a, c64_t b, c128_t acc) {
@@ -225,6 +240,15 @@ __device__ __forceinline__ c64_t shfl_idx(unsigned m, c64_t v, int src, int w) {
     return c64_t{__shfl_sync(m, v.re, src, w), __shfl_sync(m, v.im, src, w)};
 }
 template <>
+__device__ __forceinline__ c32_t shfl_idx(unsigned m, c32_t v, int src, int w) {
+    unsigned u;
+    memcpy(&u, &v, 4);
+    u = __shfl_sync(m, u, src, w);
+    c32_t r;
+    memcpy(&r, &u, 4);
+    return r;
+}
+template <>
 __device__ __forceinline__ c128_t shfl_idx(unsigned m, c128_t v, int src, int w) {
     return c128_t{__shfl_sync(m, v.re, src, w), __shfl_sync(m, v.im, src, w)};
 }
@@ -258,6 +282,9 @@ template <> struct Out<__half, float>  { static __device__ __forceinline__ __hal
 template <> struct Out<__nv_bfloat16, float> {
     static __device__ __forceinline__ __nv_bfloat16 cvt(float a) { return __float2bfloat16_rn(a); }
 };
+template <> struct Out<c32_t, c64_t>   {
+    static __device__ __forceinline__ c32_t cvt(c64_t a) { return c32_t{__float2half_rn(a.re), __float2half_rn(a.im)}; }
+};
 template <> struct Out<c64_t, c64_t>   { static __device__ __forceinline__ c64_t cvt(c64_t a) { return a; } };
 template <> struct Out<c64_t, c128_t>  {
     static __device__ __forceinline__ c64_t cvt(c128_t a) { return c64_t{(float)a.re, (float)a.im}; }
@@ -275,6 +302,7 @@ template <> struct Out<__nv_bfloat16, comp_t> {
 template <class V> __device__ __forceinline__ V vzero() { return V(0); }
 template <> __device__ __forceinline__ __half vzero<__half>() { return __float2half(0.f); }
 template <> __device__ __forceinline__ __nv_bfloat16 vzero<__nv_bfloat16>() { return __float2bfloat16(0.f); }
+template <> __device__ __forceinline__ c32_t vzero<c32_t>() { return c32_t{__float2half(0.f), __float2half(0.f)}; }
 template <> __device__ __forceinline__ c64_t vzero<c64_t>() { return c64_t{0.f, 0.f}; }
 template <> __device__ __forceinline__ c128_t vzero<c128_t>() { return c128_t{0.0, 0.0}; }
 

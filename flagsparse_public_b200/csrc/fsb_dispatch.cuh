@@ -11,6 +11,7 @@ template <class T> struct tag { using type = T; };
 //   acc_mode NATIVE : f16/bf16->f32, f32->f32, f64->f64, c64->c64, c128->c128
 //   acc_mode WIDE   : f16/bf16->f32, f32->f64, f64->f64, c64->c128, c128->c128
 //   acc_mode COMP   : f16/bf16/f32 -> compensated f32
+//   complex32 (c32) : float32 pairs in NATIVE and WIDE (as FlagSparse)
 // Output is the value type, or f32 for f16/bf16/f32 values (precision form).
 template <class F>
 int dispatch_vao(int vdt, int acc_mode, int odt, F&& f) {
@@ -50,6 +51,9 @@ int dispatch_vao(int vdt, int acc_mode, int odt, F&& f) {
     case FSB_C128:
         if (!out_same || acc_mode == FSB_ACC_COMP) break;
         return f(tag<c128_t>{}, tag<c128_t>{}, tag<c128_t>{});
+    case FSB_C32:
+        if (!out_same || acc_mode == FSB_ACC_COMP) break;
+        return f(tag<c32_t>{}, tag<c64_t>{}, tag<c32_t>{});
     default:
         break;
     }
@@ -68,7 +72,7 @@ int dispatch_idx(int dt, F&& f) {
 inline int elem_size(int dt) {
     switch (dt) {
     case FSB_F16: case FSB_BF16: return 2;
-    case FSB_F32: case FSB_I32: return 4;
+    case FSB_F32: case FSB_I32: case FSB_C32: return 4;
     case FSB_F64: case FSB_C64: case FSB_I64: return 8;
     case FSB_C128: return 16;
     default: return 0;
@@ -84,6 +88,7 @@ inline int acc_size(int vdt, int acc_mode) {
     case FSB_F64: return 8;
     case FSB_C64: return acc_mode == FSB_ACC_WIDE ? 16 : 8;
     case FSB_C128: return 16;
+    case FSB_C32: return 8;
     default: return 0;
     }
 }

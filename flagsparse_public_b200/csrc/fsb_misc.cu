@@ -116,6 +116,7 @@ static int dispatch_atomic(int vdt, int adt, F&& f) {
     if (vdt == FSB_C64 && adt == FSB_C64) return f(tag<c64_t>{}, tag<c64_t>{});
     if (vdt == FSB_C64 && adt == FSB_C128) return f(tag<c64_t>{}, tag<c128_t>{});
     if (vdt == FSB_C128 && adt == FSB_C128) return f(tag<c128_t>{}, tag<c128_t>{});
+    if (vdt == FSB_C32 && adt == FSB_C64) return f(tag<c32_t>{}, tag<c64_t>{});
     if (vdt == FSB_F16 && adt == FSB_F32) return f(tag<__half>{}, tag<float>{});
     if (vdt == FSB_BF16 && adt == FSB_F32) return f(tag<__nv_bfloat16>{}, tag<float>{});
     fsb_host::set_error("atomic route: unsupported value/accumulator pair (%d, %d)", vdt, adt);

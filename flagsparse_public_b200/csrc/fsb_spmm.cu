@@ -511,6 +511,7 @@ extern "C" int fsb_spmm_csr(const fsb_csr* A, const void* B, int64_t ldb, int64_
         case FSB_BF16: return seq_dispatch_bf16(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
         case FSB_F32: return seq_dispatch_f32(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
         case FSB_F64: return seq_dispatch_f64(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
+        case FSB_C32: return seq_dispatch_c32(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
         case FSB_C64: return seq_dispatch_c64(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
         case FSB_C128: return seq_dispatch_c128(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st);
         default:

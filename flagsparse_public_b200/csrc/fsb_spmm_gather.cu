@@ -41,6 +41,7 @@ int spmm_gather_dispatch(const fsb_csr* A, const void* B, int64_t ldb, int64_t n
     case FSB_BF16: return gather_dispatch_bf16(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st, err);
     case FSB_F32: return gather_dispatch_f32(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st, err);
     case FSB_F64: return gather_dispatch_f64(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st, err);
+    case FSB_C32: return gather_dispatch_c32(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st, err);
     case FSB_C64: return gather_dispatch_c64(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st, err);
     case FSB_C128: return gather_dispatch_c128(A, B, ldb, n_dense, C, ldc, out_dtype, acc_mode, plan, workspace, workspace_bytes, st, err);
     default:

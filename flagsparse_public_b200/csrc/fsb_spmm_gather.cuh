@@ -432,6 +432,7 @@ FSB_GATHER_DECL(gather_dispatch_f16);
 FSB_GATHER_DECL(gather_dispatch_bf16);
 FSB_GATHER_DECL(gather_dispatch_f32);
 FSB_GATHER_DECL(gather_dispatch_f64);
+FSB_GATHER_DECL(gather_dispatch_c32);
 FSB_GATHER_DECL(gather_dispatch_c64);
 FSB_GATHER_DECL(gather_dispatch_c128);
 

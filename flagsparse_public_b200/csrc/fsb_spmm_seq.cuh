@@ -396,6 +396,7 @@ FSB_SEQ_DECL(seq_dispatch_f16);
 FSB_SEQ_DECL(seq_dispatch_bf16);
 FSB_SEQ_DECL(seq_dispatch_f32);
 FSB_SEQ_DECL(seq_dispatch_f64);
+FSB_SEQ_DECL(seq_dispatch_c32);
 FSB_SEQ_DECL(seq_dispatch_c64);
 FSB_SEQ_DECL(seq_dispatch_c128);
 

@@ -144,12 +144,19 @@ def _acc_mode_for(value_dtype):
     return _nat.ACC_WIDE if value_dtype in (torch.float32, torch.complex64) else _nat.ACC_NATIVE
 
 
+def _take(values, order):
+    """values[order]; complex32 entries move as their 32-bit patterns."""
+    if _is_complex32_dtype(values.dtype):
+        return values.view(torch.int32)[order].view(values.dtype)
+    return values[order]
+
+
 def _coo_rows_to_csr(data, row, col, n_rows):
     """Order nonzeros by row (stable) and build int64 row offsets."""
     row64 = row.to(torch.int64)
     if data.numel() > 1:
         sorted_rows, order = _plan.stable_sort(row64, key_bound=n_rows)
-        data, col, row64 = data[order], col[order], sorted_rows
+        data, col, row64 = _take(data, order), col[order], sorted_rows
     indptr = _plan.sorted_keys_to_offsets(row64, n_rows)
     return data.contiguous(), col.contiguous(), indptr
 
@@ -172,6 +179,8 @@ def _triton_spmm_coo_impl(data, row, col, B, n_rows, n_dense_cols, block_n, bloc
         _plan.run_spmm(d, c, indptr, n_rows, B.shape[0], B, C, _acc_mode_for(data.dtype), plan)
         return C if C.dtype == out_dtype else C.to(out_dtype)
     acc_dtype = _spmm_coo_compute_dtype(data.dtype)
+    if _is_complex32_dtype(data.dtype):
+        acc_dtype = torch.complex64  # float32 pairs: no float16 atomics
     C_acc = torch.zeros((n_rows, n_dense_cols), dtype=acc_dtype, device=device)
     row_k = row if row.dtype == col.dtype else row.to(col.dtype)
     lib = _nat.library()

@@ -41,6 +41,8 @@ extern "C" {
 #define FSB_C128  5   /* interleaved (re, im) double pairs */
 #define FSB_I32   6
 #define FSB_I64   7
+#define FSB_C32   8   /* interleaved (re, im) float16 pairs (torch complex32),
+                         accumulated in float32 pairs                       */
 
 /* ---- accumulation modes ------------------------------------------------
  * NATIVE : f16/bf16 -> f32, f32 -> f32, f64 -> f64, c64 -> f32 pairs
@@ -87,7 +89,7 @@ typedef struct fsb_csr {
     const void* col_idx;
     const void* row_ptr;
     const void* row_map;
-    int32_t value_dtype;    /* FSB_F16 .. FSB_C128 */
+    int32_t value_dtype;    /* FSB_F16 .. FSB_C128, FSB_C32 */
     int32_t index_dtype;    /* FSB_I32 / FSB_I64, col_idx */
     int32_t ptr_dtype;      /* FSB_I32 / FSB_I64, row_ptr */
     int32_t row_map_dtype;  /* FSB_I32 / FSB_I64, row_map */

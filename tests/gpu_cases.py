@@ -11,6 +11,8 @@ def csr_from_lengths(lengths, n_cols, seed, dtype=torch.float32, index_dtype=tor
                      device="cpu"):
     """CSR with the given row lengths: sorted distinct uniform columns, U(-1,1) values."""
     lengths = torch.as_tensor(lengths, dtype=torch.int64)
+    if lengths.numel() and int(lengths.max()) > n_cols:
+        raise ValueError(f"a row of {int(lengths.max())} distinct columns needs n_cols >= that, got {n_cols}")
     g = torch.Generator().manual_seed(seed)
     n_rows = lengths.numel()
     indptr = torch.zeros(n_rows + 1, dtype=torch.int64)
