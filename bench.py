@@ -862,8 +862,126 @@ class BsrTensorCore:
         return run, nbytes, f"rows [0, {rows}) as CSR (bf16 inputs, fp32 accumulation), N = {self.n_dense}"
 
 
+class SddmmPowerlaw:
+    """SDDMM on the power-law CSR pattern of the SpMM config (262144^2,
+    Zipf(1.8) rows, mean 12): out[p] = alpha * dot(x[row(p)], y[col(p)]) +
+    beta * data[p], K = 64, float32 (float32 accumulation, as FlagSparse's
+    kernel)."""
+
+    metric = "CSR SDDMM useful HBM throughput"
+    unit = "GB/s"
+    plain_desc = "one-shot flagsparse_sddmm_csr call (pattern prepared inside every call)"
+    k = 64
+    alpha, beta = 2.0, 0.5
+
+    def __init__(self, n_rows=262144, seed=0):
+        self.n_rows = n_rows
+        self.seed = seed
+
+    def generate(self, device):
+        """Seeded inputs only (no kernel of this project runs here)."""
+        from flagsparse_public_b200 import synthetic
+
+        data, indices, indptr, shape = synthetic.zipf_powerlaw(self.n_rows, self.n_rows, alpha=1.8, mean=12.0,
+                                                               cap=20000, seed=self.seed, dtype=torch.float32,
+                                                               device=device)
+        self.A = (data, indices, indptr)
+        self.shape = shape
+        self.x = synthetic.dense_operand(shape[0], self.k, seed=self.seed + 1, dtype=torch.float32, device=device)
+        self.y = synthetic.dense_operand(shape[1], self.k, seed=self.seed + 2, dtype=torch.float32, device=device)
+        self.nnz = data.numel()
+        # per position: index, data and output word; x and y rows once each
+        self.useful_bytes = self.nnz * 12 + (shape[0] + shape[1]) * self.k * 4
+        self.flops = 2 * self.nnz * self.k
+
+    def build(self, device):
+        import flagsparse_public_b200 as fs
+
+        self.generate(device)
+        data, indices, indptr = self.A
+        self.out = torch.empty(self.nnz, dtype=torch.float32, device=device)
+        self.prepared = fs.prepare_sddmm_csr(indices, indptr, self.shape, k_hint=self.k)
+
+    def config(self):
+        return {"workload": f"csr_sddmm_powerlaw_{self.shape[0]}x{self.shape[1]}_zipf1.8_mean12_cap20000_k{self.k}"
+                            "_f32_i32",
+                "n_rows": self.shape[0], "n_cols": self.shape[1], "nnz": self.nnz, "k": self.k,
+                "alpha": self.alpha, "beta": self.beta, "global_batch": 1,
+                "useful_bytes_per_step": self.useful_bytes,
+                "l2": "flushed before every timed step (256 MiB write)", "parallelism": "replicas"}
+
+    def step(self):
+        import flagsparse_public_b200 as fs
+
+        fs.flagsparse_sddmm_csr(self.A[0], x=self.x, y=self.y, alpha=self.alpha, beta=self.beta,
+                                prepared=self.prepared, out=self.out)
+
+    def plain_step(self):
+        import flagsparse_public_b200 as fs
+
+        data, indices, indptr = self.A
+        fs.flagsparse_sddmm_csr(data, indices, indptr, self.x, self.y, self.shape, alpha=self.alpha, beta=self.beta,
+                                out=self.out)
+
+    def speedups(self, extra, ms_step, plain_ms):
+        return {}
+
+    def plan_desc(self):
+        lanes = 1
+        while lanes * 4 < self.k and lanes < 32:
+            lanes *= 2
+        return {"kind": "sddmm_subgroups", "lanes_per_position": lanes, "positions_per_batch": 4 * (32 // lanes)}
+
+    def force_plan(self, plan):
+        raise SystemExit("the SDDMM workload has no launch plans to force")
+
+    def host_inputs(self):
+        data, indices, indptr = self.A
+        self.h = [t.cpu().pin_memory() for t in (data, indices, indptr, self.x, self.y)]
+        self.h_out = torch.empty(self.out.shape, dtype=self.out.dtype).pin_memory()
+        self.h2d_bytes = sum(t.numel() * t.element_size() for t in self.h)
+        self.d2h_bytes = self.h_out.numel() * self.h_out.element_size()
+
+    def e2e_step(self, device):
+        import flagsparse_public_b200 as fs
+
+        d = [t.to(device, non_blocking=True) for t in self.h]
+        o = fs.flagsparse_sddmm_csr(d[0], d[1], d[2], d[3], d[4], self.shape, alpha=self.alpha, beta=self.beta)
+        self.h_out.copy_(o, non_blocking=True)
+
+    def fp64_error(self):
+        from tests.numerics import scaled_error
+
+        self.step()
+        data, indices, indptr = (t.cpu() for t in self.A)
+        sel = torch.arange(0, self.nnz, 97)
+        rows = torch.searchsorted(indptr, sel, right=True) - 1
+        xs, ys = self.x.cpu().double()[rows], self.y.cpu().double()[indices.long()[sel]]
+        prod = xs * ys
+        exact = self.alpha * prod.sum(1) + self.beta * data.double()[sel]
+        mag = abs(self.alpha) * prod.abs().sum(1) + abs(self.beta) * data.double()[sel].abs()
+        return {"chosen": scaled_error(self.out.cpu()[sel], exact, mag),
+                "definition": "max |o - o64| / (|alpha| sum_k |x_k y_k| + |beta data|) over every 97th position"}
+
+    def cpu_step_factory(self, threads, sample_rows=None):
+        """Oracle port of FlagSparse's SDDMM kernel (float32 accumulation) on host cores."""
+        from oracle import oracle as orc
+
+        data, indices, indptr = (t.cpu() for t in self.A)
+        rows = self.shape[0] if sample_rows is None else min(sample_rows, self.shape[0])
+        sub_ptr = indptr[: rows + 1].clone()
+        k = int(sub_ptr[-1])
+        x, y = self.x.cpu(), self.y.cpu()
+        nbytes = k * 12 + (rows + self.shape[1]) * self.k * 4
+
+        def run():
+            orc.sddmm_csr(indices[:k], sub_ptr, x[:rows], y, data[:k], self.alpha, self.beta, threads=threads)
+
+        return run, nbytes, f"rows [0, {rows}) of the workload ({k} positions), K = {self.k}"
+
+
 WORKLOADS = {"spmm_powerlaw": SpmmPowerlaw, "spmv_poisson": SpmvPoisson, "precision_banded": PrecisionBanded,
-             "batched_uneven": BatchedUneven, "bsr_tensor_core": BsrTensorCore}
+             "batched_uneven": BatchedUneven, "bsr_tensor_core": BsrTensorCore, "sddmm_powerlaw": SddmmPowerlaw}
 
 
 # ------------------------------------------------------------------ timing --

@@ -17,8 +17,12 @@ namespace fsb {
 constexpr int kSddmmThreads = 256;
 constexpr int kSddmmU = 4;
 
+// 4 resident CTAs of 256 threads per SM (64 registers): the random y-row
+// gathers are latency bound, so resident warps beat unspilled registers
+// (measured: 80 registers / 3 CTAs 0.239 ms, 64 / 4 0.188 ms, 51 / 5
+// 0.197 ms on the power-law pattern at K = 64).
 template <class V, class A, class I, int VW, int LPN_LOG2>
-__global__ void __launch_bounds__(kSddmmThreads)
+__global__ void __launch_bounds__(kSddmmThreads, 4)
 k_sddmm(const I* __restrict__ col, const int32_t* __restrict__ row_ids, int64_t nnz, const V* __restrict__ x,
         int64_t ldx, const V* __restrict__ y, int64_t ldy, int64_t k, const V* __restrict__ data,
         V* __restrict__ out, A alpha, A beta) {

@@ -11,6 +11,7 @@ non-CUDA path to fall back to (``fallback_used`` is always False).
 
 from ._common import *
 from .. import _native as _nat
+from .. import _plan
 
 SUPPORTED_SDDMM_VALUE_DTYPES = (torch.float32, torch.float64)
 
@@ -150,6 +151,7 @@ def _run_sddmm_prepared(prepared, x, y, data, alpha, beta, out):
                            _nat.ptr(out), _nat.dtype_code(x.dtype), float(alpha),
                            float(beta) if d is not None else 0.0, _nat.stream_handle(x.device))
     _nat.check(rc, "fsb_sddmm_csr")
+    _plan.LAUNCHES["count"] += 1
     return out, meta
 
 

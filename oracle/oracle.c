@@ -29,6 +29,10 @@
  *                         (spmv_csr.py:885-909), stable on (row, col).
  *   orc_seg_starts      : _seg_starts_from_sorted_rows (spmv_coo.py:312-327).
  *   orc_split_metadata  : _build_spmm_opt_split_metadata (spmm_csr.py:417-441).
+ *   orc_sddmm_csr       : _sddmm_csr_real_kernel (sddmm_csr.py:108-152):
+ *                         out[p] = alpha * dot(x[row(p)], y[col(p)]) +
+ *                         beta * data[p], the dot product accumulated in the
+ *                         value precision (float32 / float64) in K order.
  *   orc_merge_partition : checker of the merge-path partition kernel
  *                         (Merrill & Garland's merge-path search over row ends
  *                         and nonzero indices).
@@ -494,6 +498,38 @@ int orc_merge_partition(const void* ptr, int pdt, int64_t n_rows, int64_t nnz, i
         }
         coords[2 * u] = i;
         coords[2 * u + 1] = j;
+    }
+    return 0;
+}
+
+/* SDDMM on a CSR pattern (float32 or float64 values, vdt), rows in parallel. */
+int orc_sddmm_csr(const void* col, int idt, const void* ptr, int pdt, int64_t n_rows, const void* x, int64_t ldx,
+                  const void* y, int64_t ldy, int64_t k, const void* data, void* out, int vdt, double alpha,
+                  double beta, int threads) {
+    if (vdt != ORC_F32 && vdt != ORC_F64) return -2;
+#pragma omp parallel for schedule(dynamic, 256) num_threads(threads)
+    for (int64_t r = 0; r < n_rows; ++r) {
+        const int64_t s = ld_idx(ptr, pdt, r), e = ld_idx(ptr, pdt, r + 1);
+        for (int64_t q = s; q < e; ++q) {
+            const int64_t c = ld_idx(col, idt, q);
+            if (vdt == ORC_F32) {
+                const float* xr = (const float*)x + r * ldx;
+                const float* yc = (const float*)y + c * ldy;
+                float acc = 0.f;
+                for (int64_t t = 0; t < k; ++t) acc = fmaf(xr[t], yc[t], acc);
+                float v = (float)alpha * acc;
+                if (data) v += ((const float*)data)[q] * (float)beta;
+                ((float*)out)[q] = v;
+            } else {
+                const double* xr = (const double*)x + r * ldx;
+                const double* yc = (const double*)y + c * ldy;
+                double acc = 0.0;
+                for (int64_t t = 0; t < k; ++t) acc = fma(xr[t], yc[t], acc);
+                double v = alpha * acc;
+                if (data) v += ((const double*)data)[q] * beta;
+                ((double*)out)[q] = v;
+            }
+        }
     }
     return 0;
 }

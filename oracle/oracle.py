@@ -53,6 +53,8 @@ def _load():
         lib.orc_split_metadata.argtypes = [vp, vp, i64, i64, vp, vp, vp, vp]
         lib.orc_split_metadata.restype = i64
         lib.orc_merge_partition.argtypes = [vp, i32, i64, i64, i64, i64, i64, vp]
+        lib.orc_sddmm_csr.argtypes = [vp, i32, vp, i32, i64, vp, i64, vp, i64, i64, vp, vp, i32,
+                                      ctypes.c_double, ctypes.c_double, i32]
         _lib = lib
     return _lib
 
@@ -174,3 +176,19 @@ def merge_partition(indptr, n_rows, nnz, items, snap=0):
     coords = torch.empty((n_units + 1) * 2, dtype=torch.int64)
     _load().orc_merge_partition(_p(indptr), _CODES[indptr.dtype], n_rows, nnz, items, snap, n_units, _p(coords))
     return coords
+
+
+def sddmm_csr(indices, indptr, x, y, data=None, alpha=1.0, beta=0.0, threads=None):
+    """out[p] = alpha * dot(x[row(p)], y[col(p)]) + beta * data[p] on the CSR
+    pattern, accumulated in the value precision (float32 / float64)."""
+    indices, indptr, x, y = map(_host, (indices, indptr, x, y))
+    data = _host(data) if data is not None else None
+    n_rows = indptr.numel() - 1
+    out = torch.empty(indices.numel(), dtype=x.dtype)
+    rc = _load().orc_sddmm_csr(_p(indices), _CODES[indices.dtype], _p(indptr), _CODES[indptr.dtype], n_rows, _p(x),
+                               x.stride(0) if x.numel() else x.shape[1], _p(y), y.stride(0) if y.numel() else y.shape[1],
+                               x.shape[1], _p(data) if data is not None else None, _p(out), _CODES[x.dtype],
+                               float(alpha), float(beta), _threads(threads))
+    if rc != 0:
+        raise TypeError("sddmm oracle: values must be float32 or float64")
+    return out

@@ -25,6 +25,24 @@ def exact_sddmm(case):
 
 
 @pytest.mark.parametrize("name", sorted(GOLDEN))
+def test_oracle_port_matches_the_golden_outputs(name):
+    """The CPU restatement (oracle.sddmm_csr, the bench's CPU baseline) on
+    FlagSparse's own fixtures: within one value-precision rounding of the
+    reference kernel's output, condition-scaled."""
+    from oracle import oracle as orc
+
+    case = GOLDEN[name]
+    got = orc.sddmm_csr(case["indices"], case["indptr"], case["x"], case["y"],
+                        case["data"] if case["has_data"] else None, case["alpha"], case["beta"], threads=2)
+    exact, mag = exact_sddmm(case)
+    bound = 3e-5 if case["out"].dtype == torch.float32 else 1e-12
+    if got.numel():
+        err_ref = ((got.double() - case["out"].double()).abs() / mag.clamp_min(1e-300)).max().item()
+        err_exact = ((got.double() - exact).abs() / mag.clamp_min(1e-300)).max().item()
+        assert err_ref <= 2 * bound and err_exact <= bound
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN))
 def test_golden_outputs_are_within_fp64_bounds(name):
     case = GOLDEN[name]
     exact, mag = exact_sddmm(case)
