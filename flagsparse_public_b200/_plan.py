@@ -256,12 +256,16 @@ def sorted_keys_to_offsets(keys, n_bins):
     return out
 
 
+_SORT_MAX_KEYS = 2 ** 31 - 1  # fsb_stable_sort / fsb_run_starts limit
+
+
 def stable_sort(keys, key_bound=None):
     """(sorted keys, int64 permutation) of a 1-D int32 / int64 tensor, equal
     to ``torch.sort(keys, stable=True)``: fsb_stable_sort (LSD radix sort) on
     CUDA tensors, torch on CPU.  ``key_bound``: an exclusive upper bound of
     non-negative keys (fewer radix passes); None sorts the full signed width."""
-    if not keys.is_cuda:
+    if not keys.is_cuda or keys.numel() > _SORT_MAX_KEYS:
+        # host tensors, and more keys than the kernels' 32-bit positions hold
         return torch.sort(keys, stable=True)
     keys = keys.contiguous()
     n = keys.numel()
@@ -291,9 +295,11 @@ def run_starts(sorted_keys, out_dtype):
     n = sorted_keys.numel()
     if n == 0:
         return None
-    if not sorted_keys.is_cuda:
+    if not sorted_keys.is_cuda or n > _SORT_MAX_KEYS:
+        dev = sorted_keys.device
         breaks = torch.nonzero(sorted_keys[1:] != sorted_keys[:-1], as_tuple=False).flatten().to(out_dtype) + 1
-        return torch.cat([torch.zeros(1, dtype=out_dtype), breaks, torch.tensor([n], dtype=out_dtype)])
+        return torch.cat([torch.zeros(1, dtype=out_dtype, device=dev), breaks,
+                          torch.tensor([n], dtype=out_dtype, device=dev)])
     keys = sorted_keys.contiguous()
     lib = nat.library()
     starts = torch.empty(n + 1, dtype=out_dtype, device=keys.device)
