@@ -11,8 +11,9 @@ that do not depend on size, plus exact sampled rows.
   oracle, condition-scaled.
 Matrices: the power-law SpMM config (262144 x 262144, Zipf 1.8, mean 12,
 N = 64), the Poisson SpMV config (16384 x 16384, mean 16), the banded
-precision config (1,048,576 rows, 1 % rows of 8192, bf16, N = 32) and the
-tensor-core BSR config (65536 block rows x 4 blocks, N = 128, bf16)."""
+precision config (1,048,576 rows, 1 % rows of 8192, bf16, N = 32), the
+512-matrix batch config (N = 32) and the tensor-core BSR config (65536 block
+rows x 4 blocks, N = 128, bf16)."""
 
 import pytest
 import torch
@@ -126,3 +127,33 @@ def test_bsr_tensor_core_full_size():
     sd, si, sp = _sub_csr(*h, rows)
     ex, mag = orc.spmm_csr_exact(sd, si, sp, B.cpu())
     assert scaled_error(C.cpu()[rows], ex, mag) <= 3e-5
+
+
+def test_batched_512_full_size():
+    """The 512-matrix batch config (rows log-uniform in [1024, 65536], Poisson
+    lengths with mean U[2, 64], N = 32): column checksum of the stacked
+    product and exact sampled rows of every 16th matrix."""
+    import math
+
+    import numpy as np
+
+    from flagsparse_public_b200 import batched
+
+    rng = np.random.default_rng(0)
+    mats = []
+    for _ in range(512):
+        n = int(round(math.exp(rng.uniform(math.log(1024), math.log(65536)))))
+        mean = float(rng.uniform(2.0, 64.0))
+        mats.append(synthetic.poisson_uniform(n, n, mean=mean, seed=int(rng.integers(1 << 30)), device=DEV))
+    prep = batched.prepare_spmm_csr_batch(mats, 32)
+    prep.B.copy_(synthetic.dense_operand(prep.n_cols, 32, seed=1, device=DEV))
+    prep.run()
+    torch.cuda.synchronize()
+    _colsum_check(prep.C, prep.data, prep.indices, prep.B, 3e-5)
+    for i in range(0, 512, 16):
+        d, ix, ip, shape = mats[i]
+        h = [t.cpu() for t in (d, ix, ip)]
+        rows = _sampled_rows(h[2], step=997, longest=4)
+        sd, si, sp = _sub_csr(*h, rows)
+        ex, mag = orc.spmm_csr_exact(sd, si, sp, prep.b_views[i].cpu())
+        assert scaled_error(prep.c_views[i].cpu()[rows], ex, mag) <= 3e-5, i
