@@ -169,7 +169,7 @@ k_sort_downsweep(const K* __restrict__ keys_in, K in_flip, const PIn* __restrict
         __syncthreads();
         if (ok && lrank == 0u) cnt[warp][d] = (uint32_t)__popc(peers);
         __syncthreads();
-        // the owner of digit tid: exclusive prefix over the warps of this round
+        // the owner of digit tid: exclusive prefix over the warps for these 256 keys
         uint32_t acc = run;
 #pragma unroll
         for (int w = 0; w < kWarps; ++w) {

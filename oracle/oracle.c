@@ -1,9 +1,10 @@
 /*
  * oracle.c -- CPU restatement of FlagSparse's CSR/COO SpMV and SpMM path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker of the CUDA kernels in
- * flagsparse_public_b200: it is used by tests/, by __graft_entry__.smoke()
- * and by bench.py's CPU-baseline leg, never by the library itself.
+ * TEST INFRASTRUCTURE ONLY.  This file is the CPU oracle that the CUDA
+ * kernels of flagsparse_public_b200 are tested against: it is used by tests/,
+ * by __graft_entry__.smoke() and by bench.py's CPU-baseline leg, never by the
+ * library itself.
  *
  * What it restates (paths relative to the FlagSparse project root):
  *   orc_spmv_csr   : _spmv_csr_real_kernel / _spmv_csr_complex_kernel and the
@@ -18,7 +19,7 @@
  *   orc_spmm_csr   : _spmm_csr_real_kernel and the opt / alg2 / COO row-run
  *                    kernels (spmm_csr.py:92-195, :602-919,
  *                    spmm_csr_opt_alg2.py:338-629, spmm_coo.py:135-241).
- *   orc_*_exact    : the FP64 oracle the north-star error bound is stated
+ *   orc_*_exact    : the FP64 oracle the error bounds of the tests are stated
  *                    against: products split exactly (TwoProduct by fma) and
  *                    summed with Neumaier's compensated summation in double, so
  *                    the result is the exact sum rounded (almost always) once.
@@ -33,7 +34,7 @@
  *                         out[p] = alpha * dot(x[row(p)], y[col(p)]) +
  *                         beta * data[p], the dot product accumulated in the
  *                         value precision (float32 / float64) in K order.
- *   orc_merge_partition : checker of the merge-path partition kernel
+ *   orc_merge_partition : restatement of the merge-path partition kernel
  *                         (Merrill & Garland's merge-path search over row ends
  *                         and nonzero indices).
  *
