@@ -471,6 +471,7 @@ class PrecisionBanded:
     float32 forms, each with its error against FP64 of the float32 data."""
 
     metric = "bf16-value CSR SpMM useful throughput (precision form)"
+    dtype = "bf16"  # bf16 values and operand, fp32 accumulation
     unit = "GB/s"
     n_dense = 32
     plain_desc = "float32 values, float32 accumulation (same kernels)"
@@ -770,6 +771,7 @@ class BsrTensorCore:
 
     metric = "BSR 16x16 SpMM useful throughput (tensor cores)"
     unit = "GB/s"
+    dtype = "bf16"  # bf16 blocks and operand, fp32 accumulation in TMEM
     n_block_rows = 65536
     blocks_per_row = 4
     n_dense = 128
@@ -1055,7 +1057,8 @@ def run_reference(args):
     line = {
         "impl": "reference", "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic", "config": wl.config(),
+        "scaling": "weak", "vs_baseline": None, "dtype": getattr(wl, "dtype", "f32"), "data": "synthetic",
+        "config": wl.config(),
         "cpu_baseline": {"value": value, "unit": wl.unit, "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": wl.unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -1183,7 +1186,7 @@ def run_ours(args):
         line = {
             "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded generators, no dataset)",
+            "vs_baseline": None, "dtype": getattr(wl, "dtype", "f32"), "data": "synthetic (seeded generators, no dataset)",
             "config": {**wl.config(), "plan": wl.plan_desc()},
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
