@@ -218,3 +218,27 @@ def test_csr_to_bsr16_blocks_match_dense():
     for br in range(3):  # block columns sorted within each block row
         seg = bcol[int(bptr[br]):int(bptr[br + 1])]
         assert torch.all(seg[1:] > seg[:-1])
+
+
+def test_prepare_sort_wrappers_on_host_tensors():
+    """stable_sort / run_starts on host tensors: torch's stable sort and the
+    nonzero-based run starts FlagSparse uses, dtype and empty cases included."""
+    import torch
+
+    from flagsparse_public_b200 import _plan
+
+    g = torch.Generator().manual_seed(3)
+    for dtype in (torch.int32, torch.int64):
+        keys = torch.randint(0, 50, (1000,), generator=g).to(dtype)
+        k, o = _plan.stable_sort(keys, key_bound=50)
+        rk, ro = torch.sort(keys, stable=True)
+        assert torch.equal(k, rk) and torch.equal(o, ro)
+        for out_dtype in (torch.int32, torch.int64):
+            st = _plan.run_starts(k, out_dtype)
+            assert st.dtype == out_dtype
+            ref = torch.cat([torch.zeros(1, dtype=out_dtype),
+                             (torch.nonzero(k[1:] != k[:-1]).flatten() + 1).to(out_dtype),
+                             torch.tensor([k.numel()], dtype=out_dtype)])
+            assert torch.equal(st, ref)
+    assert _plan.run_starts(torch.empty(0, dtype=torch.int64), torch.int32) is None
+    assert torch.equal(_plan.run_starts(torch.tensor([7]), torch.int64), torch.tensor([0, 1]))
