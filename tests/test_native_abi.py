@@ -72,3 +72,21 @@ def test_spmm_rejects_oversized_units_on_the_host():
         rc = lib.fsb_spmm_csr(ctypes.byref(csr), 16, 8, 8, 16, 8, nat.FSB_F32, nat.ACC_NATIVE, ctypes.byref(plan), 16,
                               1 << 20, None)
         assert rc == nat.FSB_ERR_INVALID, (algo, rc)
+
+
+def test_header_constants_match_the_binding():
+    """Every #define the Python binding mirrors has the header's value."""
+    text = open(HEADER).read()
+    defines = {m.group(1): int(m.group(2)) for m in re.finditer(r"#define\s+(FSB_[A-Z0-9_]+)\s+(-?\d+)", text)}
+    mirrored = {
+        "FSB_F16": nat.FSB_F16, "FSB_BF16": nat.FSB_BF16, "FSB_F32": nat.FSB_F32, "FSB_F64": nat.FSB_F64,
+        "FSB_C64": nat.FSB_C64, "FSB_C128": nat.FSB_C128, "FSB_I32": nat.FSB_I32, "FSB_I64": nat.FSB_I64,
+        "FSB_C32": nat.FSB_C32, "FSB_ACC_NATIVE": nat.ACC_NATIVE, "FSB_ACC_WIDE": nat.ACC_WIDE,
+        "FSB_ACC_COMP": nat.ACC_COMP, "FSB_ALGO_ROWS": nat.ALGO_ROWS, "FSB_ALGO_MERGE": nat.ALGO_MERGE,
+        "FSB_ALGO_FLAT": nat.ALGO_FLAT, "FSB_ALGO_GATHER": nat.ALGO_GATHER, "FSB_ALGO_SEQ": nat.ALGO_SEQ,
+        "FSB_PLAN_TMA_GATHER": nat.PLAN_TMA_GATHER, "FSB_BSR_STAGE_TMA": nat.BSR_STAGE_TMA,
+        "FSB_BSR_STAGE_THREADS": nat.BSR_STAGE_THREADS, "FSB_ERR_UNSUPPORTED": nat.FSB_ERR_UNSUPPORTED,
+        "FSB_ERR_WORKSPACE": nat.FSB_ERR_WORKSPACE, "FSB_OK": nat.FSB_OK,
+    }
+    for name, value in mirrored.items():
+        assert defines.get(name) == value, name
