@@ -1,9 +1,8 @@
 """Generate golden vectors from FlagSparse's own SpMV/SpMM implementation.
 
-Run in a container that has the FlagSparse sources (default
-``/root/reference``, override with FLAGSPARSE_SRC=<project root>):
+Run where the FlagSparse sources are available, naming the project root:
 
-    python tests/golden/make_golden.py
+    FLAGSPARSE_SRC=<FlagSparse project root> python tests/golden/make_golden.py
 
 FlagSparse's package ``__init__`` does not import (its benchmarks module asks
 ``gather_scatter`` for a name it never defines), so the hot-path submodules are
@@ -27,7 +26,14 @@ os.environ.setdefault("TRITON_INTERPRET", "1")
 import torch  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = os.path.join(os.environ.get("FLAGSPARSE_SRC", "/root/reference"), "src", "flagsparse")
+def _src():
+    root = os.environ.get("FLAGSPARSE_SRC")
+    if not root:
+        raise SystemExit("set FLAGSPARSE_SRC to the FlagSparse project root")
+    return os.path.join(root, "src", "flagsparse")
+
+
+SRC = _src()
 
 
 def load_reference():

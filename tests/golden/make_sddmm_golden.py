@@ -1,9 +1,8 @@
 """Golden SDDMM outputs from FlagSparse's own kernel (_sddmm_csr_real_kernel
 through _run_sddmm_prepared, sddmm_csr.py:108-152, :271-348), run on CPU
-tensors under TRITON_INTERPRET=1 (FLAGSPARSE_SRC=<project root>, default
-/root/reference):
+tensors under TRITON_INTERPRET=1:
 
-    python tests/golden/make_sddmm_golden.py
+    FLAGSPARSE_SRC=<FlagSparse project root> python tests/golden/make_sddmm_golden.py
 
 Writes tests/golden/sddmm_golden.pt: per case the seeded pattern, x, y,
 data, alpha, beta and FlagSparse's output.
@@ -19,7 +18,14 @@ os.environ.setdefault("TRITON_INTERPRET", "1")
 import torch  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-SRC = os.path.join(os.environ.get("FLAGSPARSE_SRC", "/root/reference"), "src", "flagsparse")
+def _src():
+    root = os.environ.get("FLAGSPARSE_SRC")
+    if not root:
+        raise SystemExit("set FLAGSPARSE_SRC to the FlagSparse project root")
+    return os.path.join(root, "src", "flagsparse")
+
+
+SRC = _src()
 
 
 def load_sddmm():
