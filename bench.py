@@ -54,6 +54,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + timed device steps (for a profiler launch list)")
+    ap.add_argument("--only", action="store_true",
+                    help="measure the chosen workload alone (no side configurations, no selector check)")
     ap.add_argument("--plan", default=None,
                     help="force the chosen-form plan: rows:<lanes>[:<n_tile>] | merge:<items>:<snap> | "
                          "flat|gather|seq:<items>:<snap>[:<n_tile>] | g4:<items>[:<snap>[:<n_tile>]]")
@@ -111,15 +113,17 @@ def measured_peak_hbm():
 
 
 def committed_traffic(kernel_key):
-    """DRAM bytes per launch from a committed ncu summary (profiles/*.txt)."""
-    path = os.path.join(ROOT, "profiles", f"{kernel_key}.txt")
+    """DRAM bytes per launch from a committed ncu summary (profiles/*.txt) and
+    the file it was read from (an earlier cold-L2 capture of the same
+    command, not a measurement of this run); (None, None) when absent."""
+    rel = os.path.join("profiles", f"{kernel_key}.txt")
     try:
-        for line in open(path):
+        for line in open(os.path.join(ROOT, rel)):
             if line.startswith("dram_bytes_per_launch:"):
-                return float(line.split(":", 1)[1].split()[0])
+                return float(line.split(":", 1)[1].split()[0]), rel + " (committed ncu capture, cold L2)"
     except OSError:
         pass
-    return None
+    return None, None
 
 
 # ---------------------------------------------------------- clock sampling --
@@ -262,6 +266,34 @@ class SpmmPowerlaw:
 
     def force_plan(self, plan):
         self.prepared._plans[("opt", self.n_dense)] = plan
+
+    def selector_check(self, flush, steps=20, warmup=5):
+        """The plan the learned selector picked for this matrix against
+        exhaustive autotuning: every candidate timed with the bench protocol
+        (L2 flushed, CUDA events), regret = chosen / best."""
+        from flagsparse_public_b200 import _native as nat
+        from flagsparse_public_b200 import _plan, tuning
+        from flagsparse_public_b200.sparse_operations.spmm_csr import _spmm_plan_for
+
+        data, indices, indptr = self.A
+        times = {}
+        for name, factory in tuning.SPMM_CANDIDATES:
+            plan = factory()
+            C = torch.empty_like(self.C)
+
+            def run(plan=plan, C=C):
+                _plan.run_spmm(data, indices, indptr, self.shape[0], self.shape[1], self.B, C, nat.ACC_NATIVE, plan)
+
+            times[name] = _time_form(run, steps, warmup, flush, 1)
+        chosen = _spmm_plan_for(self.prepared, "opt", self.n_dense)
+        chosen_name = next((n for n, f in tuning.SPMM_CANDIDATES if f().key() == chosen.key()), None)
+        chosen_ms = _time_form(self.step, steps, warmup, flush, 1)
+        best = min(times, key=times.get)
+        return {"mode": _plan.plan_selector(), "chosen": chosen_name or chosen.describe(), "chosen_ms": chosen_ms,
+                "autotune_best": best, "autotune_best_ms": times[best], "regret": chosen_ms / times[best],
+                "candidates_ms": times,
+                "what": "learned selector's plan (prepared path) vs exhaustive autotuning over every candidate "
+                        "plan on this matrix, same timing protocol"}
 
     # end to end through the public API from pinned host memory
     def host_inputs(self):
@@ -415,9 +447,12 @@ class SpmvPoisson:
         self.graph_plain.replay()
 
     def plan_desc(self):
+        return self.graph_plan().describe()
+
+    def graph_plan(self):
         from flagsparse_public_b200.sparse_operations.spmv_csr import _spmv_plan
 
-        return _spmv_plan(self.prepared, "opt").describe()
+        return _spmv_plan(self.prepared, "opt")
 
     def force_plan(self, plan):
         self.prepared._plans[("opt", 0)] = plan
@@ -611,6 +646,13 @@ class PrecisionBanded:
             out[f"spmm_{name}_vs_fp64_same_inputs"] = scaled_error(got, ex_h, mag_h)
         self.plain_step()
         out["spmm_f32_fp32acc"] = scaled_error(self.C[rows].cpu(), exact, mag)
+        ex_v, mag_v = orc.spmv_csr_exact(*sub, self.x.cpu())
+        for dt, name in ((torch.bfloat16, "bf16"), (torch.float16, "f16")):
+            self._spmv_half(dt)
+            got = self.y[rows].cpu()
+            ex_h, mag_h = orc.spmv_csr_exact(sub[0].to(dt), sub[1], sub[2], self.x.cpu().to(dt))
+            out[f"spmv_{name}_vs_fp64_of_f32_data"] = scaled_error(got, ex_v, mag_v)
+            out[f"spmv_{name}_vs_fp64_same_inputs"] = scaled_error(got, ex_h, mag_h)
         out["definition"] = "max |c - c64| / sum_k |a_k b_k| over every 97th row"
         return out
 
@@ -706,6 +748,9 @@ class BatchedUneven:
 
     def plan_desc(self):
         return self.prep.plan.describe()
+
+    def graph_plan(self):
+        return self.prep.plan
 
     def force_plan(self, plan):
         from flagsparse_public_b200 import batched
@@ -1082,125 +1127,185 @@ def parse_plan(text):
                             n_tile=nums[2] if len(nums) > 2 else 0)
 
 
-def run_ours(args):
+def _graph_kernels(wl):
+    """Kernels one graph replay of a graph-timed workload launches."""
     from flagsparse_public_b200 import _plan
 
-    rank, world, local_rank = dist_env()
-    init_dist(world)
-    torch.cuda.set_device(local_rank)
-    device = torch.device("cuda", local_rank)
-    wl = WORKLOADS[args.workload]()
-    wl.build(device)
-    if args.plan:
-        wl.force_plan(parse_plan(args.plan))
-    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+    plan = wl.graph_plan() if hasattr(wl, "graph_plan") else None
+    per = _plan._kernels_per_call(plan) if plan is not None else 1
+    return wl.graph_iters * per
 
-    for _ in range(args.warmup):
+
+def _time_form(fn, steps, warmup, flush, world):
+    for _ in range(max(warmup, 1)):
+        fn()
+    torch.cuda.synchronize()
+    return max_over_ranks(sum(time_device_steps(fn, steps, flush)), world) / steps
+
+
+def _e2e(wl, device, steps, warmup, world):
+    """End to end through the public API with host buffers (every step's
+    host->device copies and its result's device->host copy timed)."""
+    wl.host_inputs()
+    finish = getattr(wl, "e2e_finish", None)
+    start = getattr(wl, "e2e_start", None)
+    if start is not None:
+        start(device)
+    for _ in range(max(1, min(warmup, 3))):
+        wl.e2e_step(device)
+    if finish is not None:
+        finish(device)
+    torch.cuda.synchronize()
+    barrier(world)
+    e_steps = max(3, min(steps, 20))
+    s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s.record()
+    if start is not None:
+        start(device)
+    for _ in range(e_steps):
+        wl.e2e_step(device)
+    if finish is not None:
+        finish(device)
+    e.record()
+    torch.cuda.synchronize()
+    e_ms = max_over_ranks(s.elapsed_time(e), world) / e_steps
+    check = getattr(wl, "e2e_check", None)
+    if check is not None:
+        check()
+    per_step_bytes = wl.useful_bytes / getattr(wl, "graph_iters", 1)
+    return {"value": per_step_bytes * world / (e_ms * 1e-3) / 1e9, "unit": wl.unit, "ms_per_step": e_ms,
+            "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes,
+            "what": getattr(wl, "e2e_what", "pinned host A and dense operand -> device, public one-shot API "
+                                            "(prepare + product), result -> pinned host")}
+
+
+def measure(wl, name, args, device, flush, world, rank, steps, warmup, cpu_seconds, with_e2e=True):
+    """Every figure of one workload: the chosen form (device time, L2 flushed),
+    the plain form, extra forms, end to end, FP64 error, CPU baseline."""
+    from flagsparse_public_b200 import _plan
+
+    for _ in range(warmup):
         wl.step()
     torch.cuda.synchronize()
     barrier(world)
     launches0 = _plan.LAUNCHES["count"]
-    with ClockSampler(local_rank) as clocks:
-        times = time_device_steps(wl.step, args.steps, flush)
-    graph_launches = getattr(wl, "graph_iters", 0)
+    with ClockSampler(device.index or 0) as clocks:
+        times = time_device_steps(wl.step, steps, flush)
     launches = _plan.LAUNCHES["count"] - launches0
-    if graph_launches:
+    if getattr(wl, "graph_iters", 0):
         # graph replays launch the captured kernels without passing through Python
-        launches = args.steps * graph_launches * (1 if wl.plan_desc()["kind"].endswith("rows") else 2)
+        launches = steps * _graph_kernels(wl)
     barrier(world)
-    total_ms = max_over_ranks(sum(times), world)
-    ms_step = total_ms / args.steps
+    ms_step = max_over_ranks(sum(times), world) / steps
     value = aggregate_value(wl.useful_bytes, world, ms_step)
-    if args.profile:
-        if rank == 0:
-            print(json.dumps({"profile_run": True, "ms_per_step": ms_step}), flush=True)
-        return 0
-
-    # plain (FlagSparse-compatible) form, same protocol
-    for _ in range(args.warmup):
-        wl.plain_step()
-    torch.cuda.synchronize()
-    plain_times = time_device_steps(wl.plain_step, args.steps, flush)
-    plain_ms = max_over_ranks(sum(plain_times), world) / args.steps
-    plain_value = getattr(wl, "plain_bytes", wl.useful_bytes) * world / (plain_ms * 1e-3) / 1e9
-
+    out = {"ms_per_step": ms_step, "value": value, "unit": wl.unit, "times": times, "launches": launches,
+           "clocks": clocks.summary()}
+    plain_ms = _time_form(wl.plain_step, steps, warmup, flush, world)
+    out["plain"] = {"value": getattr(wl, "plain_bytes", wl.useful_bytes) * world / (plain_ms * 1e-3) / 1e9,
+                    "unit": wl.unit, "ms_per_step": plain_ms,
+                    "form": getattr(wl, "plain_desc", "float64 accumulation (FlagSparse plain)")}
     extra = {}
     if hasattr(wl, "extra_forms"):
-        for name, (fn, nbytes) in wl.extra_forms().items():
-            for _ in range(args.warmup):
-                fn()
-            torch.cuda.synchronize()
-            ms_x = max_over_ranks(sum(time_device_steps(fn, args.steps, flush)), world) / args.steps
-            extra[name] = {"ms_per_step": ms_x, "value": nbytes * world / (ms_x * 1e-3) / 1e9, "unit": wl.unit}
+        for fname, (fn, nbytes) in wl.extra_forms().items():
+            ms_x = _time_form(fn, steps, warmup, flush, world)
+            extra[fname] = {"ms_per_step": ms_x, "value": nbytes * world / (ms_x * 1e-3) / 1e9, "unit": wl.unit}
         extra.update(wl.speedups(extra, ms_step, plain_ms))
-
-    e2e = None
-    if not args.no_e2e:
-        wl.host_inputs()
-        finish = getattr(wl, "e2e_finish", None)
-        start = getattr(wl, "e2e_start", None)
-        if start is not None:
-            start(device)
-        for _ in range(max(1, min(args.warmup, 3))):
-            wl.e2e_step(device)
-        if finish is not None:
-            finish(device)
-        torch.cuda.synchronize()
-        barrier(world)
-        e_steps = max(3, min(args.steps, 20))
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        s.record()
-        if start is not None:
-            start(device)
-        for _ in range(e_steps):
-            wl.e2e_step(device)
-        if finish is not None:
-            finish(device)
-        e.record()
-        torch.cuda.synchronize()
-        e_ms = max_over_ranks(s.elapsed_time(e), world) / e_steps
-        check = getattr(wl, "e2e_check", None)
-        if check is not None:
-            check()
-        per_step_bytes = wl.useful_bytes / getattr(wl, "graph_iters", 1)
-        e2e = {"value": per_step_bytes * world / (e_ms * 1e-3) / 1e9, "unit": wl.unit, "ms_per_step": e_ms,
-               "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes,
-               "what": getattr(wl, "e2e_what", "pinned host A and dense operand -> device, public one-shot API "
-                                               "(prepare + product), result -> pinned host")}
-
-    errors = wl.fp64_error() if rank == 0 else None
-
+    out["forms"] = extra or None
+    out["e2e"] = _e2e(wl, device, steps, warmup, world) if with_e2e else None
+    out["error_vs_fp64"] = wl.fp64_error() if rank == 0 else None
     cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+    if rank == 0 and world == 1 and cpu_seconds > 0:
         threads = cpu_threads()
         run, nbytes, sample = wl.cpu_step_factory(threads)
-        sec, reps = time_cpu(run)
+        sec, reps = time_cpu(run, min_seconds=cpu_seconds, max_seconds=3 * cpu_seconds)
         cpu = {"value": nbytes / sec / 1e9, "unit": wl.unit, "cores": threads, "kind": "port",
                "sample": f"{sample}; median of {reps} runs", "ms": sec * 1e3}
-
+    out["cpu_baseline"] = cpu
     peak, peak_kind = measured_peak_hbm()
     achieved = wl.useful_bytes / (statistics.mean(times) * 1e-3) / 1e9
-    kernel_key = f"traffic_{args.workload}"
-    traffic = committed_traffic(kernel_key)
+    traffic, source = committed_traffic(f"traffic_{name}")
+    out["roofline"] = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                       "peak_kind": peak_kind, "traffic": traffic, "traffic_source": source,
+                       "what": "useful bytes / mean CUDA-event duration of one product call"}
+    if hasattr(wl, "roofline_note"):
+        out["roofline"].update(wl.roofline_note(out))
+    out["plan"] = wl.plan_desc()
+    out["gflops"] = wl.flops * world / (ms_step * 1e-3) / 1e9
+    return out
+
+
+# The configurations measured beside the headline in the default run (one
+# JSON line): name -> (workload, steps, CPU-baseline seconds).
+SIDE_CONFIGS = (
+    ("spmv_poisson", 20, 3.0),
+    ("precision_banded", 10, 3.0),
+    ("batched_uneven", 10, 3.0),
+    ("bsr_tensor_core", 20, 3.0),
+    ("sddmm_powerlaw", 20, 3.0),
+)
+
+
+def _compact(m):
+    keep = ("ms_per_step", "value", "unit", "plain", "forms", "e2e", "error_vs_fp64", "cpu_baseline", "roofline",
+            "plan", "gflops", "launches", "clocks")
+    return {k: m[k] for k in keep if k in m}
+
+
+def run_ours(args):
+    rank, world, local_rank = dist_env()
+    init_dist(world)
+    torch.cuda.set_device(local_rank)
+    device = torch.device("cuda", local_rank)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device=device)
+    wl = WORKLOADS[args.workload]()
+    wl.build(device)
+    if args.plan:
+        wl.force_plan(parse_plan(args.plan))
+
+    if args.profile:
+        for _ in range(args.warmup):
+            wl.step()
+        torch.cuda.synchronize()
+        times = time_device_steps(wl.step, args.steps, flush)
+        if rank == 0:
+            print(json.dumps({"profile_run": True, "ms_per_step": sum(times) / len(times)}), flush=True)
+        return 0
+
+    head = measure(wl, args.workload, args, device, flush, world, rank, args.steps, args.warmup,
+                   0.0 if args.no_cpu else 10.0, with_e2e=not args.no_e2e)
+    selector = wl.selector_check(flush) if hasattr(wl, "selector_check") and rank == 0 and not args.only else None
+    config = {**wl.config(), "plan": head["plan"]}
+    del wl
+    torch.cuda.empty_cache()
+
+    configs = {}
+    if not args.only:
+        for name, steps, cpu_s in SIDE_CONFIGS:
+            if name == args.workload:
+                continue
+            side = WORKLOADS[name]()
+            side.build(device)
+            m = measure(side, name, args, device, flush, world, rank, min(args.steps, steps), max(3, args.warmup),
+                        0.0 if args.no_cpu else cpu_s, with_e2e=not args.no_e2e)
+            configs[name] = {"metric": side.metric, "dtype": getattr(side, "dtype", "f32"), "config": side.config(),
+                             **_compact(m)}
+            del side
+            torch.cuda.empty_cache()
+
     if rank == 0:
         line = {
-            "metric": wl.metric, "value": value, "unit": wl.unit, "n_gpus": world, "steps": args.steps,
-            "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": getattr(wl, "dtype", "f32"), "data": "synthetic (seeded generators, no dataset)",
-            "config": {**wl.config(), "plan": wl.plan_desc()},
-            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
-                         "what": "useful bytes / mean CUDA-event duration of one product call"},
-            "plain": {"value": plain_value, "unit": wl.unit, "ms_per_step": plain_ms,
-                      "frac": plain_value / world / peak, "form": getattr(wl, "plain_desc",
-                                                                          "float64 accumulation (FlagSparse plain)")},
-            "forms": extra or None,
-            "error_vs_fp64": errors,
-            "e2e": e2e,
-            "cpu_baseline": cpu,
-            "gpu_launches": launches,
-            "clocks": clocks.summary(),
-            "gflops": wl.flops * world / (ms_step * 1e-3) / 1e9,
+            "metric": WORKLOADS[args.workload].metric, "value": head["value"], "unit": head["unit"],
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": head["ms_per_step"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": getattr(WORKLOADS[args.workload], "dtype", "f32"),
+            "data": "synthetic (seeded generators, no dataset)", "config": config,
+            "roofline": head["roofline"], "plain": head["plain"], "forms": head["forms"],
+            "error_vs_fp64": head["error_vs_fp64"], "e2e": head["e2e"], "cpu_baseline": head["cpu_baseline"],
+            "gpu_launches": head["launches"] + sum(c.get("launches", 0) for c in configs.values()),
+            "gpu_launches_headline": head["launches"],
+            "clocks": head["clocks"], "gflops": head["gflops"],
+            "selector": selector,
+            "configs": configs or None,
         }
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -73,6 +73,40 @@ class FsbPlan(ctypes.Structure):
         ("comp_threshold", ctypes.c_int64),
         ("grid_blocks", ctypes.c_int32),
         ("flags", ctypes.c_int32),
+        ("unit_runs", ctypes.c_void_p),
+        ("tickets", ctypes.c_void_p),
+        ("ticket_slots", ctypes.c_int64),
+    ]
+
+
+class FsbStruct(ctypes.Structure):
+    _fields_ = [
+        ("run_col", ctypes.c_void_p),
+        ("run_off", ctypes.c_void_p),
+        ("run_len", ctypes.c_void_p),
+        ("tile_base", ctypes.c_void_p),
+        ("tile_span", ctypes.c_void_p),
+        ("max_span", ctypes.c_int32),
+        ("chunk_nnz", ctypes.c_int32),
+        ("n_long", ctypes.c_int64),
+        ("long_rows", ctypes.c_void_p),
+        ("n_chunks", ctypes.c_int64),
+        ("chunk_row", ctypes.c_void_p),
+        ("chunk_ptr", ctypes.c_void_p),
+        ("xblock", ctypes.c_int32),
+        ("reserved", ctypes.c_int32),
+        ("n_xblocks", ctypes.c_int64),
+        ("seg_ptr", ctypes.c_void_p),
+        ("seg_val", ctypes.c_void_p),
+        ("seg_off", ctypes.c_void_p),
+        ("lt_groups", ctypes.c_int64),
+        ("lt_col_blocks", ctypes.c_int64),
+        ("lt_rec_cap", ctypes.c_int32),
+        ("reserved2", ctypes.c_int32),
+        ("lt_rec", ctypes.c_void_p),
+        ("lt_seg_start", ctypes.c_void_p),
+        ("lt_seg_len", ctypes.c_void_p),
+        ("lt_row_start", ctypes.c_void_p),
     ]
 
 
@@ -91,6 +125,11 @@ _SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, ctypes.c_int64,
          ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
+    ),
+    "fsb_merge_runs": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_void_p],
     ),
     "fsb_spmv_csr": (
         ctypes.c_int,
@@ -117,6 +156,27 @@ _SIGNATURES = {
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_int64,
          ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int,
          ctypes.c_void_p],
+    ),
+    "fsb_struct_rows": (
+        ctypes.c_int,
+        [ctypes.POINTER(FsbCsr), ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+         ctypes.c_void_p],
+    ),
+    "fsb_struct_tiles": (
+        ctypes.c_int,
+        [ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+         ctypes.c_void_p],
+    ),
+    "fsb_struct_workspace_bytes": (ctypes.c_int64, [ctypes.c_int, ctypes.POINTER(FsbStruct), ctypes.c_int64]),
+    "fsb_struct_spmv": (
+        ctypes.c_int,
+        [ctypes.POINTER(FsbCsr), ctypes.POINTER(FsbStruct), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
+         ctypes.c_int64, ctypes.c_void_p],
+    ),
+    "fsb_struct_spmm": (
+        ctypes.c_int,
+        [ctypes.POINTER(FsbCsr), ctypes.POINTER(FsbStruct), ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64,
+         ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
     ),
     "fsb_bsr_spmm_tc": (
         ctypes.c_int,
@@ -258,7 +318,7 @@ def make_csr(values, col_idx, row_ptr, n_rows, n_cols, row_map=None):
 
 
 def make_plan(algo, lanes=32, items_per_unit=0, n_tile=0, coords=None, n_units=0, row_cap=0, comp_threshold=0,
-              grid_blocks=0, flags=0):
+              grid_blocks=0, flags=0, runs=None, tickets=None):
     p = FsbPlan()
     p.algo = int(algo)
     p.lanes = int(lanes)
@@ -270,4 +330,7 @@ def make_plan(algo, lanes=32, items_per_unit=0, n_tile=0, coords=None, n_units=0
     p.comp_threshold = int(comp_threshold)
     p.grid_blocks = int(grid_blocks)
     p.flags = int(flags)
+    p.unit_runs = runs.data_ptr() if runs is not None and runs.numel() > 0 else 0
+    p.tickets = tickets.data_ptr() if tickets is not None and tickets.numel() > 0 else 0
+    p.ticket_slots = int(tickets.numel()) if tickets is not None else 0
     return p

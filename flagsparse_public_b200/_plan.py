@@ -17,15 +17,21 @@ import torch
 from . import _native as nat
 
 SPMV_MERGE_THREADS = 128
-SPMM_SNAP_DEFAULT = 0
+# SEQ plans move unit boundaries that fall inside rows shorter than this many
+# nonzeros back to the row start: only longer rows are split across units
+# (power-law SpMM: 169 us snapped against 172 us unsnapped at 128 items).
+SPMM_SNAP_DEFAULT = 64
 
 # Kernels launched by run_spmv / run_spmm since import (partition launches
-# excluded): one per call for row groups, two (tiles + carry fix-up) for merge.
+# excluded): one per call for row groups and for the SpMM merge-path kernel
+# that finishes split rows itself, two (tiles + carry fix-up) otherwise.
 LAUNCHES = {"count": 0}
 
 
 def _kernels_per_call(plan):
-    return 1 if plan.algo == nat.ALGO_ROWS else 2
+    if plan.algo == nat.ALGO_ROWS:
+        return 1
+    return 1 if plan.in_kernel_finish() else 2
 
 
 class MatrixStats:
@@ -64,7 +70,7 @@ class KernelPlan:
     """One launch configuration of fsb_spmv_csr / fsb_spmm_csr."""
 
     __slots__ = ("algo", "lanes", "items_per_unit", "n_tile", "snap", "coords", "n_units", "row_cap",
-                 "comp_threshold", "fallback_ok", "grid_blocks", "flags")
+                 "comp_threshold", "fallback_ok", "grid_blocks", "flags", "runs", "tickets")
 
     def __init__(self, algo, lanes=32, items_per_unit=0, n_tile=0, snap=0, row_cap=0, comp_threshold=0,
                  fallback_ok=False, grid_blocks=0, flags=0):
@@ -80,6 +86,17 @@ class KernelPlan:
         self.fallback_ok = bool(fallback_ok)
         self.grid_blocks = int(grid_blocks)
         self.flags = int(flags)
+        self.runs = None
+        self.tickets = None
+
+    def _seq_registers(self):
+        return self.algo == nat.ALGO_SEQ and not (self.flags & nat.PLAN_TMA_GATHER)
+
+    def in_kernel_finish(self):
+        """Whether split rows finish inside the SEQ kernel (unit runs + ticket
+        counters) rather than in the separate carry fix-up: decided once per
+        partition by ensure_runs."""
+        return self._seq_registers() and self.runs is not None and self.runs is not False
 
     def as_flat(self):
         """The register-staged flat plan over the same merge-path units."""
@@ -125,10 +142,57 @@ class KernelPlan:
         self.coords = coords
         self.n_units = n_units
 
+    def ensure_runs(self, row_ptr, n_rows, n_dense):
+        """SEQ plans: the unit runs of the partition (once) and, when split
+        rows finish in the kernel, zero-filled ticket counters for one per
+        unit and column tile of an n_dense-wide call (the kernel returns them
+        to zero).  Each unit holding part of a split row takes an atomic
+        ticket at its end, which pays off against the separate fix-up launch
+        only while such units are few: at most IN_KERNEL_FINISH_MAX of them
+        (one host read, once per partition; decided outside stream capture,
+        the fix-up runs meanwhile)."""
+        if not self._seq_registers():
+            return
+        if self.runs is None:
+            if row_ptr.is_cuda and torch.cuda.is_current_stream_capturing():
+                return
+            runs = torch.empty(max(self.n_units, 1) * 2, dtype=torch.int64, device=row_ptr.device)
+            contributors = 0
+            if self.n_units > 0:
+                rc = nat.library().fsb_merge_runs(nat.ptr(row_ptr), nat.dtype_code(row_ptr.dtype), int(n_rows),
+                                                  nat.ptr(self.coords), self.n_units, nat.ptr(runs),
+                                                  nat.stream_handle(row_ptr.device))
+                nat.check(rc, "fsb_merge_runs")
+                contributors = int((runs.view(-1, 2)[: self.n_units, 0] >= 0).sum())
+            self.runs = runs if contributors <= IN_KERNEL_FINISH_MAX else False
+        if self.runs is False:
+            return
+        need = self.n_units * ticket_col_tiles(n_dense, self.n_tile)
+        if self.tickets is None or self.tickets.numel() < need:
+            self.tickets = torch.zeros(max(need, 1), dtype=torch.int32, device=row_ptr.device)
+
     def c_plan(self):
+        finish = self.in_kernel_finish()
         return nat.make_plan(self.algo, lanes=self.lanes, items_per_unit=self.items_per_unit, n_tile=self.n_tile,
                              coords=self.coords, n_units=self.n_units, row_cap=self.row_cap,
-                             comp_threshold=self.comp_threshold, grid_blocks=self.grid_blocks, flags=self.flags)
+                             comp_threshold=self.comp_threshold, grid_blocks=self.grid_blocks, flags=self.flags,
+                             runs=self.runs if finish else None, tickets=self.tickets if finish else None)
+
+
+# Split rows finish inside the SEQ kernel while at most this many units hold
+# parts of them (power-law SpMM: 10 K - 24 K such units, 5 - 10 us faster than
+# the separate fix-up; banded matrix: 152 K, 66 us slower).
+IN_KERNEL_FINISH_MAX = 32768
+
+
+def ticket_col_tiles(n_dense, n_tile=0):
+    """Upper bound of the column tiles of a SEQ launch: a tile spans
+    (lane vector) x (lanes per nonzero) >= min(target width, 32) columns."""
+    n_dense = int(n_dense)
+    if n_dense <= 0:
+        return 1
+    width = int(n_tile) if n_tile > 0 else n_dense
+    return -(-n_dense // max(1, min(width, 32)))
 
 
 def _pow2_clamp(v, lo, hi):
@@ -175,7 +239,7 @@ def default_spmm_plan(stats, n_dense, dtype, row_cap=0):
     segment cap is requested."""
     if row_cap > 0 or stats.n_rows == 0:
         return KernelPlan(nat.ALGO_ROWS, lanes=32, row_cap=row_cap)
-    return KernelPlan(nat.ALGO_SEQ, items_per_unit=seq_items_per_unit(stats))
+    return KernelPlan(nat.ALGO_SEQ, items_per_unit=seq_items_per_unit(stats), snap=SPMM_SNAP_DEFAULT)
 
 
 # How the prepared SpMM paths pick their plan: "learned" (the shipped
@@ -394,6 +458,7 @@ def run_spmm(values, col_idx, row_ptr, n_rows, n_cols, B, C, acc_mode, plan, row
         plan.flags &= ~nat.PLAN_TMA_GATHER
     plan.ensure_coords(row_ptr, n_rows, values.numel())
     n_dense = int(B.shape[1])
+    plan.ensure_runs(row_ptr, n_rows, n_dense)
     cm = nat.make_csr(values, col_idx, row_ptr, n_rows, n_cols, row_map)
     cp = plan.c_plan()
     out_code = nat.dtype_code(C.dtype)

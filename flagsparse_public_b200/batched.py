@@ -26,7 +26,8 @@ SM_COUNT = _plan.SM_COUNT
 
 
 def _seq(items, grid=0, n_tile=0):
-    return lambda: _plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=items, n_tile=n_tile, grid_blocks=grid)
+    return lambda: _plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=items, n_tile=n_tile, grid_blocks=grid,
+                                    snap=_plan.SPMM_SNAP_DEFAULT)
 
 
 # (name, factory): unit sizes x {one CTA per 4 units, persistent 8 / 16 CTAs per SM}

@@ -229,20 +229,35 @@ __device__ __forceinline__ uint64_t smem_desc_sw128(uint32_t addr, uint32_t lbo,
     return smem_desc(addr, lbo, sbo) | (2ull << 61);
 }
 
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+// L2 policies of the persistent kernel: B slices are re-read by every block
+// row that names their block column (keep them), blocks and C pass once.
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar,
+                                            uint64_t pol) {
     asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
-            "r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, "
+        "%3}], [%4], %5;" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar), "l"(pol)
         : "memory");
 }
 
-__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, int c4, uint32_t bar) {
+__device__ __forceinline__ void tma_load_5d(uint32_t dst, const CUtensorMap* map, int c4, uint32_t bar,
+                                            uint64_t pol) {
     asm volatile(
-        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, %5, "
-        "%6}], [%7];" ::"r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(0), "r"(0), "r"(c4), "r"(bar)
+        "cp.async.bulk.tensor.5d.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint [%0], [%1, {%2, "
+        "%3, %4, %5, %6}], [%7], %8;" ::"r"(dst),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(0), "r"(0), "r"(0), "r"(0), "r"(c4), "r"(bar), "l"(pol)
         : "memory");
+}
+
+// C store that bypasses L1 and enters L2 as evict-first.
+__device__ __forceinline__ void st_evict_first(float* p, float v, uint64_t pol) {
+    asm volatile("st.global.L1::no_allocate.L2::cache_hint.f32 [%0], %1, %2;" ::"l"(p), "f"(v), "l"(pol) : "memory");
 }
 
 // Persistent, warp-specialised pipeline.  Each CTA takes block rows
@@ -330,6 +345,7 @@ k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const __grid_constant__
             }
             uint32_t issued = 0, g = 0;
             bool ok = true;
+            const uint64_t keep_b = policy_evict_last(), pass_once = policy_evict_first();
             auto issue_more = [&](uint32_t upto) {  // blocks [issued, upto] of this CTA, as far as they exist
                 while (ok && issued <= upto) {
                     while (ib >= ie && ir < n_block_rows) {
@@ -348,9 +364,9 @@ k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const __grid_constant__
                     const uint32_t bar = smem_u32(&full[s]);
                     tma::mbar_arrive_expect_tx(bar, kStageTx);
                     const int y = (int)(idx(bcol[ib]) * 16);
-                    tma_load_2d(smem_u32(&sa[s][0]), &bmap, (int)c0, y, bar);
-                    tma_load_2d(smem_u32(&sa[s][kTmaBoxBytes]), &bmap, (int)c0 + kTmaBoxCols, y, bar);
-                    tma_load_5d(smem_u32(&sb[s][0]), &amap, (int)ib, bar);
+                    tma_load_2d(smem_u32(&sa[s][0]), &bmap, (int)c0, y, bar, keep_b);
+                    tma_load_2d(smem_u32(&sa[s][kTmaBoxBytes]), &bmap, (int)c0 + kTmaBoxCols, y, bar, keep_b);
+                    tma_load_5d(smem_u32(&sb[s][0]), &amap, (int)ib, bar, pass_once);
                     ++issued;
                     ++ib;
                 }
@@ -406,6 +422,7 @@ k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const __grid_constant__
         __syncwarp();
     } else {
         // epilogue warps: TMEM lane quarter `warp` = dense columns c0 + 32 warp + lane
+        const uint64_t c_pol = policy_evict_first();
         int64_t k = 0;
         for (int64_t r = blockIdx.x; r < n_block_rows; r += stride, ++k) {
             const uint32_t buf = (uint32_t)(k & 1);
@@ -447,7 +464,7 @@ k_bsr_spmm_tma(const __grid_constant__ CUtensorMap bmap, const __grid_constant__
 #pragma unroll
                 for (int n = 0; n < 16; ++n) {
                     const int64_t row = r * 16 + n;
-                    if (row < n_rows) __stcs(C + row * ldc + c0 + m, __uint_as_float(d[n]));
+                    if (row < n_rows) st_evict_first(C + row * ldc + c0 + m, __uint_as_float(d[n]), c_pol);
                 }
             }
         }

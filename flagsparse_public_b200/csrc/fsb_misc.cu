@@ -106,6 +106,22 @@ extern "C" int fsb_merge_partition(const void* row_ptr, int ptr_dtype, int64_t n
     });
 }
 
+extern "C" int fsb_merge_runs(const void* row_ptr, int ptr_dtype, int64_t n_rows, const int64_t* unit_coords,
+                              int64_t n_units, int64_t* unit_runs, void* stream) {
+    if (!row_ptr || !unit_coords || !unit_runs || n_rows < 0 || n_units < 0) {
+        fsb_host::set_error("fsb_merge_runs: bad arguments");
+        return FSB_ERR_INVALID;
+    }
+    if (n_units == 0) return FSB_OK;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    return dispatch_idx(ptr_dtype, [&](auto tp) -> int {
+        using P = typename decltype(tp)::type;
+        k_merge_runs<P><<<(unsigned)ceil_div(n_units, 256), 256, 0, st>>>(static_cast<const P*>(row_ptr), n_rows,
+                                                                         unit_coords, n_units, unit_runs);
+        return fsb_host::check_launch("k_merge_runs");
+    });
+}
+
 // Value/accumulator pairs of the atomic routes: the accumulator buffer is the
 // value type or its wide type.
 template <class F>

@@ -17,8 +17,14 @@
 // kernel small.  B loads carry an L2 evict-last policy: B rows are gathered
 // many times while the values and column indices stream through once.
 //
-// Split rows finish through the carries shared with the other merge-path SpMM
-// kernels (k_spmm_merge_fixup).
+// Split rows (rows spread over several units) finish in one of two ways.
+// With the plan's unit runs and ticket counters, inside this kernel: each
+// unit holding part of such a row stores its partial (the carry at its end,
+// the head partial where the row ends), then takes a ticket on the row's
+// counter; the unit drawing the last ticket adds the row's partials in unit
+// order and stores the row.  Nothing waits, so nothing can hang, and the sums
+// are those of the separate fix-up kernel (k_spmm_merge_fixup), which runs
+// instead when the plan carries no runs.
 #pragma once
 #include <type_traits>
 
@@ -30,7 +36,9 @@ namespace fsb {
 // (128 x blocks)): 8 (64 registers) while a lane's accumulators take at most
 // 16 bytes, 6 (80 registers) up to 48 bytes (block-compensated rows add a
 // 4-byte partial per element), else 4.  Gathers are latency bound, so
-// resident warps are worth more than the few bytes ptxas spills at 64.
+// resident warps are worth more than the few bytes ptxas spills at 64 (fewer
+// resident warps with twice or four times the loads per batch measured
+// slower on the power-law SpMM: 191 and 229 us against 170 us).
 template <class V, class A, int VW> struct SeqMinBlocks {
     static constexpr int acc_bytes =
         (int)sizeof(A) * VW + ((is_comp_acc<A>::value && sizeof(V) == 2) ? 4 * VW : 0);
@@ -45,13 +53,93 @@ template <class V, class A, int VW, int NPAR> struct SeqBatch {
     static constexpr int value = by_elems * NPAR > 32 ? 32 / NPAR : by_elems;
 };
 
+// Load of a partial written by another CTA in this launch: L2 only (no stale
+// L1 line can answer it).
+template <class A>
+__device__ __forceinline__ A ld_partial(const A* p) {
+    using R = typename raw_type<sizeof(A)>::T;
+    R r = __ldcg(reinterpret_cast<const R*>(p));
+    A out;
+    memcpy(&out, &r, sizeof(A));
+    return out;
+}
+
+// Whole warp, after its lanes stored their partial of a split row: one ticket
+// on the row's counter; true on the warp that drew the last of `count`
+// tickets, which then resets the counter for the next call.  The lanes'
+// stores are ordered before lane 0's ticket by the warp barrier; the ticket is
+// an acquire-release atomic, so the finisher's loads after it (and after the
+// broadcast) see every contributor's partial.
+__device__ __forceinline__ bool seq_take_ticket(int* slot, int count, int lane) {
+    __syncwarp();
+    int last = 0;
+    if (lane == 0) {
+        int old;
+        asm volatile("atom.acq_rel.gpu.global.add.s32 %0, [%1], 1;" : "=r"(old) : "l"(slot) : "memory");
+        last = old == count - 1;
+        if (last) *slot = 0;
+    }
+    last = __shfl_sync(0xffffffffu, last, 0);
+    __syncwarp();  // the other lanes' loads follow lane 0's acquire
+    return last != 0;
+}
+
+// The finishing unit's lanes (sub-group 0) add the split row's partials in
+// unit order -- carries of units first .. last - 1, then the head partial of
+// unit last, as k_spmm_merge_fixup does -- and store the row.
+template <class A, class O, class I, class P, int VW>
+__device__ __forceinline__ void seq_finish_row(int64_t first, int64_t last, int64_t row, const A* carry_val,
+                                               const A* head_val, int64_t n_dense, int64_t c0, const P* ptr,
+                                               const I* row_map, O* C, int64_t ldc) {
+    A sum[VW];
+    const A* p = carry_val + first * n_dense + c0;
+#pragma unroll
+    for (int w = 0; w < VW; ++w) sum[w] = ld_partial(p + w);
+    for (int64_t u = first + 1; u < last; ++u) {
+        p = carry_val + u * n_dense + c0;
+#pragma unroll
+        for (int w = 0; w < VW; ++w) sum[w] = acc_add(sum[w], ld_partial(p + w));
+    }
+    p = head_val + last * n_dense + c0;
+#pragma unroll
+    for (int w = 0; w < VW; ++w) sum[w] = acc_add(sum[w], ld_partial(p + w));
+    const int64_t out_row = row_map ? idx(row_map[idx(ptr[row])]) : row;
+    store_row<O, A, VW>(C, ldc, out_row, c0, sum);
+}
+
+// Whole warp, once at the end of a unit whose partials are stored: tickets
+// for the split row the unit continued and ended (its head partial) and for
+// the row open at its end (its carry); finishes the rows whose last ticket it
+// drew.  Not inlined: kept out of the register allocation of the unit loop.
+template <class A, class O, class I, class P, int VW>
+__device__ __noinline__ void seq_unit_tickets(int64_t unit, int64_t r0, int64_t r1, bool head, bool open,
+                                              int lane, bool finisher_lane, int64_t c0, const int64_t* runs,
+                                              int* tix, const A* carry_val, const A* head_val, int64_t n_dense,
+                                              const P* ptr, const I* row_map, O* C, int64_t ldc) {
+    for (int job = 0; job < 2; ++job) {
+        int64_t first = -1, last = -1, row = 0;
+        if (job == 0 && head) {
+            first = runs[2 * unit - 2];
+            last = unit;
+            row = r0;
+        } else if (job == 1 && open) {
+            first = runs[2 * unit];
+            last = runs[2 * unit + 1];
+            row = r1;
+        }
+        if (first >= 0 && last > first && seq_take_ticket(tix + first, (int)(last - first + 1), lane) &&
+            finisher_lane)
+            seq_finish_row<A, O, I, P, VW>(first, last, row, carry_val, head_val, n_dense, c0, ptr, row_map, C, ldc);
+    }
+}
+
 template <class V, class A, class O, class I, class P, int VW, int LPN_LOG2, bool ADDR32>
 __global__ void __launch_bounds__(kSpmmThreads, SeqMinBlocks<V, A, VW>::value)
 k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __restrict__ ptr,
            const I* __restrict__ row_map, const V* __restrict__ B, int64_t ldb, O* __restrict__ C, int64_t ldc,
            int64_t n_rows, int64_t n_dense, const int64_t* __restrict__ coords, int64_t n_units,
            int64_t comp_threshold, int64_t* __restrict__ carry_row, A* __restrict__ carry_val,
-           A* __restrict__ head_val) {
+           A* __restrict__ head_val, const int64_t* __restrict__ runs, int* __restrict__ tickets) {
     constexpr int kNoEnd = 0x7fffffff;
     constexpr int LPN = 1 << LPN_LOG2;
     constexpr int NPAR = 32 >> LPN_LOG2;
@@ -264,7 +352,15 @@ k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __rest
                 }
             }
         }
-        if (blockIdx.y == 0 && lane == 0) carry_row[unit] = open ? r1 : -1;
+        if (runs) {
+            // the split rows this unit holds parts of: the one it continued
+            // and ended (head partial) and the one open at its end (carry)
+            seq_unit_tickets<A, O, I, P, VW>(unit, r0, r1, continued && r1 > r0, open, lane, sub == 0 && col_ok, c0,
+                                             runs, tickets + (int64_t)blockIdx.y * n_units, carry_val, head_val,
+                                             n_dense, ptr, row_map, C, ldc);
+        } else if (blockIdx.y == 0 && lane == 0) {
+            carry_row[unit] = open ? r1 : -1;
+        }
     }
 }
 
@@ -278,15 +374,18 @@ constexpr int seq_max_vw() {
 template <class V, class A, class O, class I, class P, int VW>
 void launch_seq_vw(int lpn_log2, bool addr32, dim3 g, cudaStream_t st, const V* val, const I* col, const P* ptr,
                    const I* rmap, const V* B, int64_t ldb, O* C, int64_t ldc, int64_t n_rows, int64_t n_dense,
-                   const int64_t* coords, int64_t n_units, int64_t thr, int64_t* carry_row, A* cv, A* hv) {
+                   const int64_t* coords, int64_t n_units, int64_t thr, int64_t* carry_row, A* cv, A* hv,
+                   const int64_t* runs, int* tickets) {
+#define FSB_SEQ_KERNEL(L, A32)                                                                                  \
+    k_spmm_seq<V, A, O, I, P, VW, L, A32><<<g, kSpmmThreads, 0, st>>>(                                          \
+        val, col, ptr, rmap, B, ldb, C, ldc, n_rows, n_dense, coords, n_units, thr, carry_row, cv, hv, runs,    \
+        tickets)
 #define FSB_SEQ_LAUNCH(L)                                                                                         \
     if (lpn_log2 == L) {                                                                                          \
         if (addr32)                                                                                               \
-            k_spmm_seq<V, A, O, I, P, VW, L, true><<<g, kSpmmThreads, 0, st>>>(                                   \
-                val, col, ptr, rmap, B, ldb, C, ldc, n_rows, n_dense, coords, n_units, thr, carry_row, cv, hv);   \
+            FSB_SEQ_KERNEL(L, true);                                                                              \
         else                                                                                                      \
-            k_spmm_seq<V, A, O, I, P, VW, L, false><<<g, kSpmmThreads, 0, st>>>(                                  \
-                val, col, ptr, rmap, B, ldb, C, ldc, n_rows, n_dense, coords, n_units, thr, carry_row, cv, hv);   \
+            FSB_SEQ_KERNEL(L, false);                                                                             \
         return;                                                                                                   \
     }
     FSB_SEQ_LAUNCH(0)
@@ -296,6 +395,7 @@ void launch_seq_vw(int lpn_log2, bool addr32, dim3 g, cudaStream_t st, const V* 
     FSB_SEQ_LAUNCH(4)
     FSB_SEQ_LAUNCH(5)
 #undef FSB_SEQ_LAUNCH
+#undef FSB_SEQ_KERNEL
 }
 
 template <class V, class A, class O, class I, class P>
@@ -346,16 +446,23 @@ int launch_seq(const fsb_csr* Am, const V* val, const I* col, const P* ptr, cons
     // tile, its warps striding over the units
     const int64_t grid = plan->grid_blocks > 0 && plan->grid_blocks < blocks ? plan->grid_blocks : blocks;
     dim3 g((unsigned)grid, (unsigned)col_tiles);
+    // split rows finish inside the kernel when the plan brings the unit runs
+    // and enough ticket counters (one per unit and column tile)
+    const bool in_kernel = plan->unit_runs && plan->tickets && plan->ticket_slots >= n_units * col_tiles;
+    const int64_t* runs = in_kernel ? plan->unit_runs : nullptr;
+    int* tickets = in_kernel ? reinterpret_cast<int*>(plan->tickets) : nullptr;
     if (vw == kMaxVW)
         launch_seq_vw<V, A, O, I, P, kMaxVW>(lpn_log2, addr32, g, st, val, col, ptr, rmap, B, ldb, C, ldc, Am->n_rows,
-                                             n_dense, plan->unit_coords, n_units, thr, ms.carry_row, cv, hv);
+                                             n_dense, plan->unit_coords, n_units, thr, ms.carry_row, cv, hv, runs,
+                                             tickets);
     if constexpr (kMaxVW > 1) {
         if (vw == 1)
             launch_seq_vw<V, A, O, I, P, 1>(lpn_log2, addr32, g, st, val, col, ptr, rmap, B, ldb, C, ldc, Am->n_rows,
-                                            n_dense, plan->unit_coords, n_units, thr, ms.carry_row, cv, hv);
+                                            n_dense, plan->unit_coords, n_units, thr, ms.carry_row, cv, hv, runs,
+                                            tickets);
     }
     int rc = fsb_host::check_launch("k_spmm_seq");
-    if (rc) return rc;
+    if (rc || in_kernel) return rc;
     k_spmm_merge_fixup<A, O, I, P><<<(unsigned)blocks, kSpmmThreads, 0, st>>>(
         ms.carry_row, static_cast<const A*>(ms.carry_val), static_cast<const A*>(ms.head_val), n_units, n_dense, ptr,
         rmap, C, ldc);

@@ -351,9 +351,11 @@ extern "C" int fsb_spmv_csr(const fsb_csr* A, const void* x, void* y, int out_dt
 // kernels overlap on the GPU (for example on two streams) race on it, so
 // callers must order such calls.  Nothing in the array has to start at zero:
 // each call writes the coordinates and every tile's carry slot before they
-// are read.  The first call on a device resolves the array's device address
-// (cudaGetSymbolAddress) with that device current; that first call should
-// come before any stream capture.
+// are read.  The first call in a CUDA context (the device's primary context,
+// or a host framework's own context current on the calling thread) resolves
+// the array's device address in that context (cudaGetSymbolAddress) and
+// caches it per context; that first call should come before any stream
+// capture.
 constexpr int64_t kNoAllocMaxTiles = 16384;
 constexpr int64_t kNoAllocCoordBytes = ((kNoAllocMaxTiles + 1) * 2 * 8 + 255) / 256 * 256;
 constexpr int64_t kNoAllocBytes = kNoAllocCoordBytes + (kNoAllocMaxTiles * 8 + 255) / 256 * 256 +
@@ -361,29 +363,68 @@ constexpr int64_t kNoAllocBytes = kNoAllocCoordBytes + (kNoAllocMaxTiles * 8 + 2
 static __device__ __align__(256) unsigned char g_spmv_noalloc_scratch[kNoAllocBytes];
 
 namespace {
-constexpr int kMaxDevices = 64;
+// The array's device address belongs to the CUDA context that was current
+// when it was resolved: a plug-in may run inside its host framework's own
+// driver context rather than the device's primary context.  Addresses are
+// therefore cached per context (cuCtxGetCurrent, reached through the
+// runtime's driver entry-point query), not per device ordinal.
+using CtxGetCurrentFn = int (*)(void**);
+constexpr int kMaxContexts = 64;
 std::mutex g_noalloc_mutex;
-void* g_noalloc_ptr[kMaxDevices] = {};
+void* g_noalloc_ctx[kMaxContexts] = {};
+void* g_noalloc_ptr[kMaxContexts] = {};
+int g_noalloc_used = 0;
 
-// Device address of the scratch array for the current device (set up once).
+CtxGetCurrentFn ctx_get_current() {
+    static std::once_flag once;
+    static CtxGetCurrentFn fn = nullptr;
+    std::call_once(once, [] {
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<CtxGetCurrentFn>(p);
+    });
+    return fn;
+}
+
+// Device address of the scratch array in the current context (resolved on
+// the first call made in that context).
 int noalloc_scratch(void** out) {
-    int dev = 0;
-    cudaError_t e = cudaGetDevice(&dev);
-    if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
-        fsb_host::set_error("fsb_spmv_csr_noalloc: no usable current device (%s)", cudaGetErrorString(e));
+    CtxGetCurrentFn get_ctx = ctx_get_current();
+    if (!get_ctx) {
+        fsb_host::set_error("fsb_spmv_csr_noalloc: cuCtxGetCurrent is not available");
         return FSB_ERR_LAUNCH;
     }
+    void* ctx = nullptr;
+    if (get_ctx(&ctx) != 0) ctx = nullptr;
     std::lock_guard<std::mutex> lock(g_noalloc_mutex);
-    if (!g_noalloc_ptr[dev]) {
-        void* p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_spmv_noalloc_scratch);
-        if (e != cudaSuccess || !p) {
-            fsb_host::set_error("fsb_spmv_csr_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
-            return FSB_ERR_LAUNCH;
+    if (ctx) {
+        for (int i = 0; i < g_noalloc_used; ++i) {
+            if (g_noalloc_ctx[i] == ctx) {
+                *out = g_noalloc_ptr[i];
+                return FSB_OK;
+            }
         }
-        g_noalloc_ptr[dev] = p;
     }
-    *out = g_noalloc_ptr[dev];
+    // First call in this context (or no context current yet: the runtime
+    // then makes the current device's primary context current here).
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_spmv_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+        fsb_host::set_error("fsb_spmv_csr_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+        return FSB_ERR_LAUNCH;
+    }
+    if (!ctx && (get_ctx(&ctx) != 0 || !ctx)) {
+        fsb_host::set_error("fsb_spmv_csr_noalloc: no current CUDA context");
+        return FSB_ERR_LAUNCH;
+    }
+    if (g_noalloc_used < kMaxContexts) {
+        g_noalloc_ctx[g_noalloc_used] = ctx;
+        g_noalloc_ptr[g_noalloc_used] = p;
+        ++g_noalloc_used;
+    }
+    *out = p;
     return FSB_OK;
 }
 }  // namespace

@@ -18,19 +18,23 @@ max |y - y64| / sum_k |a_k x_k|.
 from ._common import *
 from .. import _native as _nat
 from .. import _plan
+from .. import _structured
 from .spmv_csr import _prepare_spmv_csr_matrix
 
 MIXED_VALUE_DTYPES = (torch.bfloat16, torch.float16)
 COMPENSATE_ABOVE = 4096
+LAYOUTS = ("auto", "csr", "structured")
 
 
 class PreparedCsrMixed:
-    """Validated half-precision CSR and its cached launch plans."""
+    """Validated half-precision CSR, its cached launch plans and (layout
+    "auto" / "structured") its structured form."""
 
     __slots__ = ("data", "kernel_indices", "kernel_indptr", "shape", "n_rows", "n_cols", "max_row_nnz",
-                 "compensate_above", "_stats", "_plans")
+                 "compensate_above", "layout", "_stats", "_plans", "_struct")
 
-    def __init__(self, data, kernel_indices, kernel_indptr, shape, n_rows, n_cols, max_row_nnz, compensate_above):
+    def __init__(self, data, kernel_indices, kernel_indptr, shape, n_rows, n_cols, max_row_nnz, compensate_above,
+                 layout="auto"):
         self.data = data
         self.kernel_indices = kernel_indices
         self.kernel_indptr = kernel_indptr
@@ -39,18 +43,44 @@ class PreparedCsrMixed:
         self.n_cols = int(n_cols)
         self.max_row_nnz = int(max_row_nnz)
         self.compensate_above = int(compensate_above)
+        self.layout = layout
         self._stats = None
         self._plans = {}
+        self._struct = None
 
 
-def prepare_csr_mixed(data, indices, indptr, shape, compensate_above=COMPENSATE_ABOVE):
-    """Validate a bfloat16 / float16 CSR matrix for the precision form."""
+def prepare_csr_mixed(data, indices, indptr, shape, compensate_above=COMPENSATE_ABOVE, layout="auto"):
+    """Validate a bfloat16 / float16 CSR matrix for the precision form.
+
+    ``layout``: "csr" runs the products on the CSR kernels; "structured" on the
+    structured form (runs of consecutive columns on the tensor cores, long
+    rows in compensated chunks); "auto" builds the structured form and uses it
+    when runs and long rows hold at least half of the nonzeros."""
     if torch.is_tensor(data) and data.dtype not in MIXED_VALUE_DTYPES:
         raise TypeError("precision form needs bfloat16 or float16 values")
     if int(compensate_above) < 0:
         raise ValueError("compensate_above must be non-negative")
+    if layout not in LAYOUTS:
+        raise ValueError(f"layout must be one of {LAYOUTS}")
     data, kidx, kptr, n_rows, n_cols, _lens, max_row = _prepare_spmv_csr_matrix(data, indices, indptr, shape)
-    return PreparedCsrMixed(data, kidx, kptr, shape, n_rows, n_cols, max_row, compensate_above)
+    p = PreparedCsrMixed(data, kidx, kptr, shape, n_rows, n_cols, max_row, compensate_above, layout)
+    if layout != "csr":
+        _structured_form(p)
+    return p
+
+
+def _structured_form(prepared):
+    """The structured form when this matrix runs on it, else None.  Rows of
+    more than the structured form's long-row threshold accumulate compensated
+    there, so a compensation threshold below it keeps the CSR kernels."""
+    if prepared._struct is None:
+        use = False
+        if prepared.layout != "csr" and prepared.n_rows > 0 and prepared.compensate_above >= _structured.LONG_MIN:
+            form = _structured.build(prepared.data, prepared.kernel_indices, prepared.kernel_indptr,
+                                     prepared.n_rows, prepared.n_cols)
+            use = form if (prepared.layout == "structured" or form.worthwhile()) else False
+        prepared._struct = use
+    return prepared._struct or None
 
 
 def _stats(prepared):
@@ -84,11 +114,11 @@ def _mixed_plan(prepared, kind, n_dense=0, operands=None):
     return plan
 
 
-def _resolve(data, indices, indptr, shape, prepared, compensate_above):
+def _resolve(data, indices, indptr, shape, prepared, compensate_above, layout="auto"):
     if prepared is None:
         if any(a is None for a in (data, indices, indptr, shape)):
             raise ValueError("data, indices, indptr, and shape are required when prepared is not provided")
-        prepared = prepare_csr_mixed(data, indices, indptr, shape, compensate_above=compensate_above)
+        prepared = prepare_csr_mixed(data, indices, indptr, shape, compensate_above=compensate_above, layout=layout)
     elif not isinstance(prepared, PreparedCsrMixed):
         raise TypeError("prepared must be a PreparedCsrMixed instance")
     return prepared
@@ -122,9 +152,9 @@ def _error_vs_fp64(prepared, dense, result):
 
 
 def flagsparse_spmv_csr_mixed(data=None, indices=None, indptr=None, x=None, shape=None, prepared=None, out=None,
-                              compensate_above=COMPENSATE_ABOVE, return_time=False, return_error=False):
+                              compensate_above=COMPENSATE_ABOVE, return_time=False, return_error=False, layout="auto"):
     """y = A x with half-precision A and x, float32 accumulation and result."""
-    prepared = _resolve(data, indices, indptr, shape, prepared, compensate_above)
+    prepared = _resolve(data, indices, indptr, shape, prepared, compensate_above, layout)
     x = _check_dense(x, "x", prepared, 1)
     if out is not None and (out.dtype != torch.float32 or out.shape != (prepared.n_rows,) or not out.is_contiguous()
                             or out.device != prepared.data.device):
@@ -135,8 +165,13 @@ def flagsparse_spmv_csr_mixed(data=None, indices=None, indptr=None, x=None, shap
         torch.cuda.synchronize()
         t0 = time.perf_counter()
     if prepared.n_rows:
-        _plan.run_spmv(prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
-                       prepared.n_cols, x, y, _acc_mode(prepared), _mixed_plan(prepared, "spmv"))
+        form = _structured_form(prepared)
+        if form is not None:
+            _structured.spmv(form, prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
+                             prepared.n_cols, x, y)
+        else:
+            _plan.run_spmv(prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
+                           prepared.n_cols, x, y, _acc_mode(prepared), _mixed_plan(prepared, "spmv"))
     res = [y]
     if return_time:
         torch.cuda.synchronize()
@@ -147,9 +182,9 @@ def flagsparse_spmv_csr_mixed(data=None, indices=None, indptr=None, x=None, shap
 
 
 def flagsparse_spmm_csr_mixed(data=None, indices=None, indptr=None, B=None, shape=None, prepared=None, out=None,
-                              compensate_above=COMPENSATE_ABOVE, return_time=False, return_error=False):
+                              compensate_above=COMPENSATE_ABOVE, return_time=False, return_error=False, layout="auto"):
     """C = A B with half-precision A and B (row-major), float32 accumulation and result."""
-    prepared = _resolve(data, indices, indptr, shape, prepared, compensate_above)
+    prepared = _resolve(data, indices, indptr, shape, prepared, compensate_above, layout)
     B = _check_dense(B, "B", prepared, 2)
     n_dense = int(B.shape[1])
     if out is not None and (out.dtype != torch.float32 or out.shape != (prepared.n_rows, n_dense)
@@ -162,8 +197,13 @@ def flagsparse_spmm_csr_mixed(data=None, indices=None, indptr=None, B=None, shap
         torch.cuda.synchronize()
         t0 = time.perf_counter()
     if prepared.n_rows and n_dense:
-        _plan.run_spmm(prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
-                       prepared.n_cols, B, C, _acc_mode(prepared), _mixed_plan(prepared, "spmm", n_dense, (B, C)))
+        form = _structured_form(prepared)
+        if form is not None and _structured.spmm_supported(form, B, C):
+            _structured.spmm(form, prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
+                             prepared.n_cols, B, C)
+        else:
+            _plan.run_spmm(prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
+                           prepared.n_cols, B, C, _acc_mode(prepared), _mixed_plan(prepared, "spmm", n_dense, (B, C)))
     res = [C]
     if return_time:
         torch.cuda.synchronize()

@@ -62,7 +62,7 @@ def _merge(items, snap):
 
 
 def _seq(items, n_tile=0):
-    return lambda: _plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=items, n_tile=n_tile)
+    return lambda: _plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=items, n_tile=n_tile, snap=_plan.SPMM_SNAP_DEFAULT)
 
 
 # (name, plan factory); the order is the network's output order.

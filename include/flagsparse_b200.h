@@ -21,7 +21,7 @@
 extern "C" {
 #endif
 
-#define FSB_ABI_VERSION 1
+#define FSB_ABI_VERSION 2
 
 /* ---- status codes ------------------------------------------------------ */
 #define FSB_OK               0
@@ -115,6 +115,19 @@ typedef struct fsb_plan {
     int32_t grid_blocks;     /* ROWS, SEQ: CTAs to launch (SEQ: a persistent grid
                                 striding over the units), 0 = automatic           */
     int32_t flags;           /* FSB_PLAN_* bits, 0 = none                          */
+    /* SEQ only, optional (null: split rows finish in a second kernel).
+     * unit_runs [n_units * 2] from fsb_merge_runs for the same unit_coords;
+     * tickets: ticket_slots int32 counters, zero-filled by the caller once
+     * when allocated, at least n_units * (column tiles of the call) of them.
+     * With both, the kernel finishes each split row itself: every unit that
+     * holds part of the row stores its partial, then takes a ticket; the unit
+     * drawing the last ticket adds the row's partials in unit order (the same
+     * sums as the second kernel) and stores the row.  No unit ever waits.  The
+     * counters return to zero by the end of every call; calls sharing one
+     * ticket array must not overlap on the GPU.                            */
+    const int64_t* unit_runs;
+    int32_t* tickets;
+    int64_t ticket_slots;
 } fsb_plan;
 
 int         fsb_abi_version(void);
@@ -151,6 +164,17 @@ int fsb_merge_partition(const void* row_ptr, int ptr_dtype, int64_t n_rows,
                         int64_t snap_threshold, int64_t* unit_coords,
                         int64_t n_units, void* stream);
 
+/* Split-row runs of a merge-path partition (unit_coords from
+ * fsb_merge_partition for the same row_ptr): for every unit u whose end falls
+ * inside a row r (after at least one of r's nonzeros), unit_runs[2*u] is the
+ * first and unit_runs[2*u+1] the last unit holding part of r (the last one
+ * holds r's end); -1, -1 for the other units.  Computed once per partition
+ * (binary searches over the coordinates).  Replaces the per-call host loop
+ * over long rows of _build_spmm_opt_split_metadata (spmm_csr.py:417-441).  */
+int fsb_merge_runs(const void* row_ptr, int ptr_dtype, int64_t n_rows,
+                   const int64_t* unit_coords, int64_t n_units,
+                   int64_t* unit_runs, void* stream);
+
 /* Allocation-free merge-path SpMV, y = A x, for callers that cannot allocate
  * device memory (a C program or plug-in handed device pointers by a host
  * framework that owns all device memory, or a latency-critical loop that
@@ -161,8 +185,10 @@ int fsb_merge_partition(const void* row_ptr, int ptr_dtype, int64_t n_rows,
  * library (about 0.9 MB, held by every GPU that loads the library until
  * exit): at most 16384 tiles, i.e. n_rows + nnz <= 16384 * items_per_unit,
  * else FSB_ERR_LIMIT.  Calls whose kernels overlap on the GPU race on the
- * shared array.  The first call on a device resolves the array's address
- * with that device current and should come before any stream capture.     */
+ * shared array.  The first call in a CUDA context (the device's primary
+ * context, or a host framework's own context current on the calling thread)
+ * resolves the array's address in that context and caches it per context;
+ * that first call should come before any stream capture.                 */
 int fsb_spmv_csr_noalloc(const fsb_csr* A, const void* x, void* y, int out_dtype,
                          int acc_mode, int32_t items_per_unit, void* stream);
 
@@ -236,6 +262,78 @@ int64_t fsb_run_starts_workspace_bytes(int64_t n);
 int fsb_run_starts(const void* sorted_keys, int key_dtype, int64_t n,
                    void* starts, int starts_dtype, int64_t* count,
                    void* workspace, int64_t workspace_bytes, void* stream);
+
+/* ---- structured form: runs of consecutive columns and long rows -------- *
+ * Descriptors added to a CSR matrix (which stays as it is) for the precision
+ * form's SpMV / SpMM on matrices whose nonzeros sit mostly in runs of
+ * consecutive columns (a band) or in a few long rows.  All device arrays.   */
+typedef struct fsb_struct {
+    const int32_t* run_col;   /* [n_rows] first column of the row's run       */
+    const int32_t* run_off;   /* [n_rows] offset of the run inside the row    */
+    const int32_t* run_len;   /* [n_rows] run length, 0: none, -1: long row   */
+    const int64_t* tile_base; /* [ceil(n_rows / 128)] first column of the
+                                 tile's run span                               */
+    const int32_t* tile_span; /* [ceil(n_rows / 128)] span width, a multiple
+                                 of 16, at most 256 (0: no runs)              */
+    int32_t max_span;         /* largest tile_span                            */
+    int32_t chunk_nnz;        /* SpMM: nonzeros per chunk of a long row       */
+    int64_t n_long;           /* long rows                                    */
+    const int32_t* long_rows; /* [n_long] their indices                       */
+    int64_t n_chunks;         /* SpMM: chunks of the long rows                */
+    const int32_t* chunk_row; /* [n_chunks] long-row position of each chunk   */
+    const int64_t* chunk_ptr; /* [n_long + 1] first chunk of each long row    */
+    int32_t xblock;           /* SpMV: columns of x per block (<= 65536)      */
+    int32_t reserved;
+    int64_t n_xblocks;        /* SpMV: ceil(n_cols / xblock)                  */
+    const int64_t* seg_ptr;   /* [n_xblocks * n_long + 1] start of the (block,
+                                 long row) segments of the regrouped nonzeros */
+    const void* seg_val;      /* values of the long rows, by (block, row)     */
+    const uint16_t* seg_off;  /* their columns minus the block's first column */
+    /* SpMM, optional (lt_rec null: chunks): the long rows in tiles of 512
+     * rows x 1024 columns.  Per (row group, column block) segment: records
+     * (value bits | column inside the block << 16), ordered by row, padded
+     * to a multiple of 4, starting at lt_seg_start (a multiple of 4), with
+     * 520 16-bit per-row record starts (513 used).                          */
+    int64_t lt_groups;          /* ceil(n_long / 512)                        */
+    int64_t lt_col_blocks;      /* ceil(n_cols / 1024)                       */
+    int32_t lt_rec_cap;         /* longest padded segment, in records        */
+    int32_t reserved2;
+    const uint32_t* lt_rec;
+    const int64_t* lt_seg_start; /* [lt_groups * lt_col_blocks]              */
+    const int32_t* lt_seg_len;   /* [lt_groups * lt_col_blocks] padded        */
+    const uint16_t* lt_row_start;/* [lt_groups * lt_col_blocks * 520]         */
+} fsb_struct;
+
+/* Per-row descriptors: the longest run of consecutive columns of each row of
+ * at most long_min nonzeros (run_len < min_run: no run); longer rows get
+ * run_len = -1.  No FlagSparse counterpart (FlagSparse buckets rows by length
+ * only, spmv_csr.py:345-391, spmm_csr.py:444-477).                          */
+int fsb_struct_rows(const fsb_csr* A, int64_t long_min, int32_t min_run,
+                    int32_t* run_col, int32_t* run_off, int32_t* run_len,
+                    void* stream);
+/* Per-tile spans (tiles of 128 rows); runs that do not fit a 256-column span
+ * starting at the tile's first run column are dropped (run_len, run_off set
+ * to 0).                                                                    */
+int fsb_struct_tiles(int64_t n_rows, const int32_t* run_col, int32_t* run_off,
+                     int32_t* run_len, int64_t* tile_base, int32_t* tile_span,
+                     void* stream);
+/* Workspace bytes of fsb_struct_spmv (is_spmm 0) / fsb_struct_spmm.         */
+int64_t fsb_struct_workspace_bytes(int is_spmm, const fsb_struct* S,
+                                   int64_t n_dense);
+/* y (float32) = A x, A and x float16 / bfloat16, float32 accumulation (long
+ * rows compensated).  Replaces, for the precision form, the bucket kernels
+ * of FlagSparse's opt SpMV (spmv_csr.py:393-440).                           */
+int fsb_struct_spmv(const fsb_csr* A, const fsb_struct* S, const void* x,
+                    float* y, void* workspace, int64_t workspace_bytes,
+                    void* stream);
+/* C (float32) = A B, B row-major float16 / bfloat16 with n_dense of 16, 32
+ * or 64; runs on the tensor cores (tcgen05, float32 accumulators in tensor
+ * memory), long rows in chunks (compensated).  B and C 16-byte aligned, ldb
+ * a multiple of 8, ldc of 4.  Replaces, for the precision form, the bucket
+ * and split kernels of FlagSparse's opt SpMM (spmm_csr.py:1252-1360).       */
+int fsb_struct_spmm(const fsb_csr* A, const fsb_struct* S, const void* B,
+                    int64_t ldb, int64_t n_dense, float* C, int64_t ldc,
+                    void* workspace, int64_t workspace_bytes, void* stream);
 
 /* ---- block-sparse SpMM on the tensor cores ----------------------------- *
  * C (float32, n_rows x n_dense, row stride ldc) = A B for A in BSR form with

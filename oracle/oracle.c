@@ -37,6 +37,9 @@
  *   orc_merge_partition : restatement of the merge-path partition kernel
  *                         (Merrill & Garland's merge-path search over row ends
  *                         and nonzero indices).
+ *   orc_merge_runs      : the split-row runs of a partition (which units hold
+ *                         parts of one row), by a linear walk -- the unit-level
+ *                         form of the long-row split metadata above.
  *
  * Sums run in row order, one nonzero after the other; the reference's Triton
  * kernels sum 256-lane tiles as trees, so agreement is to rounding, not bits,
@@ -499,6 +502,45 @@ int orc_merge_partition(const void* ptr, int pdt, int64_t n_rows, int64_t nnz, i
         }
         coords[2 * u] = i;
         coords[2 * u + 1] = j;
+    }
+    return 0;
+}
+
+/* Split-row runs of a merge-path partition, by a linear walk over the units:
+ * unit u is open when its end (r, k) lies inside row r after r's start and
+ * after u's own start; its run is the maximal sequence of consecutive units
+ * open on row r, extended by the unit holding r's end.  runs[2u] / [2u + 1]
+ * = first / last unit of that run, -1 for units that are not open.  (The
+ * reference splits long rows on the host, spmm_csr.py:417-441; this is the
+ * same bookkeeping for merge-path units.) */
+int orc_merge_runs(const void* ptr, int pdt, int64_t n_rows, const int64_t* coords, int64_t n_units,
+                   int64_t* runs) {
+    for (int64_t u = 0; u < n_units; ++u) {
+        runs[2 * u] = -1;
+        runs[2 * u + 1] = -1;
+    }
+    int64_t u = 0;
+    while (u < n_units) {
+        const int64_t r = coords[2 * u + 2], k1 = coords[2 * u + 3], k0 = coords[2 * u + 1];
+        int open = 0;
+        if (r < n_rows) {
+            const int64_t s = ld_idx(ptr, pdt, r);
+            open = k1 > (s > k0 ? s : k0);
+        }
+        if (!open) {
+            ++u;
+            continue;
+        }
+        /* u opens a run on row r: every following unit that ends on row r
+         * continues it, the first unit ending past row r closes it */
+        int64_t v = u;
+        while (v < n_units && coords[2 * v + 2] == r) ++v;
+        /* v: first unit whose end row is past r (holds r's end) */
+        for (int64_t w = u; w < v; ++w) {
+            runs[2 * w] = u;
+            runs[2 * w + 1] = v;
+        }
+        u = v;
     }
     return 0;
 }

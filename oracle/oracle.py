@@ -53,6 +53,7 @@ def _load():
         lib.orc_split_metadata.argtypes = [vp, vp, i64, i64, vp, vp, vp, vp]
         lib.orc_split_metadata.restype = i64
         lib.orc_merge_partition.argtypes = [vp, i32, i64, i64, i64, i64, i64, vp]
+        lib.orc_merge_runs.argtypes = [vp, i32, i64, vp, i64, vp]
         lib.orc_sddmm_csr.argtypes = [vp, i32, vp, i32, i64, vp, i64, vp, i64, i64, vp, vp, i32,
                                       ctypes.c_double, ctypes.c_double, i32]
         _lib = lib
@@ -169,6 +170,17 @@ def split_metadata(indptr, long_rows, part_nnz):
     return rows[:n], starts[:n], ends[:n], rpp
 
 
+def merge_runs(indptr, n_rows, coords):
+    """(first, last) unit of the split-row run of each unit's open row, -1 when
+    the unit's end is not inside a row (int64 [n_units * 2])."""
+    indptr, coords = _host(indptr), _host(coords).to(torch.int64)
+    n_units = coords.numel() // 2 - 1
+    runs = torch.empty(max(n_units, 0) * 2, dtype=torch.int64)
+    if n_units > 0:
+        _load().orc_merge_runs(_p(indptr), _CODES[indptr.dtype], int(n_rows), _p(coords), n_units, _p(runs))
+    return runs
+
+
 def merge_partition(indptr, n_rows, nnz, items, snap=0):
     indptr = _host(indptr)
     total = n_rows + nnz
@@ -192,3 +204,58 @@ def sddmm_csr(indices, indptr, x, y, data=None, alpha=1.0, beta=0.0, threads=Non
     if rc != 0:
         raise TypeError("sddmm oracle: values must be float32 or float64")
     return out
+
+
+def struct_rows(indices, indptr, long_min, min_run):
+    """Per-row descriptors of the structured form (pure Python, small cases):
+    the row's longest run of consecutive columns -- (first column, offset in
+    the row, length), the first run on ties, (0, 0, 0) when shorter than
+    min_run -- or (0, 0, -1) for rows of more than long_min nonzeros."""
+    indices, indptr = _host(indices).tolist(), _host(indptr).tolist()
+    out = []
+    for r in range(len(indptr) - 1):
+        s, e = indptr[r], indptr[r + 1]
+        if e - s > long_min:
+            out.append((0, 0, -1))
+            continue
+        best_len, best_start, start = 0, 0, 0
+        for k in range(1, e - s + 1):
+            if k == e - s or indices[s + k] != indices[s + k - 1] + 1:
+                if k - start > best_len:
+                    best_len, best_start = k - start, start
+                start = k
+        if best_len >= min_run and best_len > 0:
+            out.append((indices[s + best_start], best_start, best_len))
+        else:
+            out.append((0, 0, 0))
+    t = torch.tensor(out, dtype=torch.int32).view(-1, 3)
+    return t[:, 0].contiguous(), t[:, 1].contiguous(), t[:, 2].contiguous()
+
+
+def struct_tiles(run_col, run_off, run_len, tile_rows=128, span_max=256):
+    """Tile spans of the structured form: per tile of tile_rows rows, the
+    smallest run column; runs ending more than span_max columns past it are
+    dropped (length and offset set to 0); width rounded up to 16.  Returns
+    (tile_base, tile_span, run_off, run_len) (the last two updated)."""
+    run_col = _host(run_col).tolist()
+    run_off, run_len = _host(run_off).clone(), _host(run_len).clone()
+    n = len(run_col)
+    bases, spans = [], []
+    for t0 in range(0, max(n, 1), tile_rows):
+        rows = [r for r in range(t0, min(n, t0 + tile_rows)) if int(run_len[r]) > 0]
+        if not rows:
+            bases.append(0)
+            spans.append(0)
+            continue
+        lo = min(run_col[r] for r in rows)
+        hi = lo
+        for r in rows:
+            end = run_col[r] + int(run_len[r])
+            if end - lo > span_max:
+                run_len[r] = 0
+                run_off[r] = 0
+            else:
+                hi = max(hi, end)
+        bases.append(lo)
+        spans.append((hi - lo + 15) // 16 * 16)
+    return (torch.tensor(bases, dtype=torch.int64), torch.tensor(spans, dtype=torch.int32), run_off, run_len)

@@ -72,6 +72,8 @@ def spmm_plans():
               for ipu, snap, nt in ((16, 0, 0), (100, 0, 0), (256, 128, 0), (2048, 0, 0), (128, 64, 32), (77, 0, 8))]
     # persistent grids: one and three CTAs striding over every unit
     plans += [_plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=ipu, grid_blocks=g) for ipu, g in ((16, 1), (64, 3))]
+    # snapped units (only rows of at least 64 nonzeros split)
+    plans += [_plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=ipu, snap=64) for ipu in (100, 128)]
     # B rows staged by TMA gather4: short units (ring slots reused across
     # units), long units (the ring wraps many times), snapped units, column
     # tiles, one persistent CTA

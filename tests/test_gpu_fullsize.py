@@ -7,11 +7,13 @@ that do not depend on size, plus exact sampled rows.
   (float32 accumulation 3e-5, float64 accumulation of float32 data 1e-5).
 * Linearity: A (2 B1 - 3 B2) against 2 A B1 - 3 A B2, entrywise within
   eps * (2 |A||B1| + 3 |A||B2|) (x 2 for the two sides).
-* Sampled rows: every 4096th row and the longest rows against the FP64
-  oracle, condition-scaled.
+* Rows against the FP64 oracle, condition-scaled: every row of the
+  power-law SpMM and of the Poisson SpMV; sampled rows (a fixed stride plus
+  the longest rows) of the larger configurations.
 Matrices: the power-law SpMM config (262144 x 262144, Zipf 1.8, mean 12,
 N = 64), the Poisson SpMV config (16384 x 16384, mean 16), the banded
-precision config (1,048,576 rows, 1 % rows of 8192, bf16, N = 32), the
+precision config (1,048,576 rows, 1 % rows of 8192, bf16 and fp16, SpMM with
+N = 32 and SpMV), the
 512-matrix batch config (N = 32) and the tensor-core BSR config (65536 block
 rows x 4 blocks, N = 128, bf16)."""
 
@@ -76,16 +78,15 @@ def test_powerlaw_spmm_full_size(powerlaw):
     absA = fs.flagsparse_spmm_csr_opt(data.abs(), indices, indptr, 2 * B1.abs() + 3 * B2.abs(), shape)
     lin = ((C12.double() - (2 * C1.double() - 3 * C2.double())).abs() / absA.double().clamp(min=1e-30))
     assert float(lin.max()) <= 2 * 3e-5 * 1.01
-    # exact sampled rows (every 4096th and the longest)
+    # every row against the FP64 oracle (3.1 M nonzeros x 64 columns on the host)
     h = [t.cpu() for t in (data, indices, indptr)]
-    rows = _sampled_rows(h[2])
-    sd, si, sp = _sub_csr(*h, rows)
-    ex, mag = orc.spmm_csr_exact(sd, si, sp, B1.cpu())
-    assert scaled_error(C1.cpu()[rows], ex, mag) <= 3e-5
-    # the FlagSparse-compatible plain form (float64 accumulation)
+    ex, mag = orc.spmm_csr_exact(*h, B1.cpu())
+    assert scaled_error(C1.cpu(), ex, mag) <= 3e-5
+    # the FlagSparse-compatible plain form (float64 accumulation): within one
+    # float32 rounding of the FP64 result on every row
     Cp = fs.flagsparse_spmm_csr(data, indices, indptr, B1, shape)
     _colsum_check(Cp, data, indices, B1, 1e-5)
-    assert scaled_error(Cp.cpu()[rows], ex, mag) <= 1e-5
+    assert scaled_error(Cp.cpu(), ex, mag) <= 1e-5
 
 
 def test_poisson_spmv_full_size_exact():
@@ -97,23 +98,49 @@ def test_poisson_spmv_full_size_exact():
         assert scaled_error(y, ex, mag) <= bound
 
 
-def test_banded_precision_spmm_full_size():
-    data, indices, indptr, shape = synthetic.banded_plus_random(seed=0, dtype=torch.bfloat16, device=DEV)
-    B = synthetic.dense_operand(shape[1], 32, seed=1, dtype=torch.bfloat16, device=DEV)
+@pytest.fixture(scope="module", params=[torch.bfloat16, torch.float16], ids=["bf16", "f16"])
+def banded(request):
+    dt = request.param
+    data, indices, indptr, shape = synthetic.banded_plus_random(seed=0, dtype=dt, device=DEV)
     p = fs.prepare_csr_mixed(data, indices, indptr, shape)
-    C = fs.flagsparse_spmm_csr_mixed(B=B, prepared=p)
-    assert C.dtype == torch.float32
-    _colsum_check(C, data, indices, B, 3e-5)
     h = [t.cpu() for t in (data, indices, indptr)]
     lens = h[2][1:] - h[2][:-1]
     long_rows = torch.nonzero(lens > 4096).flatten()[::64]
-    rows = torch.unique(torch.cat([_sampled_rows(h[2], step=65536), long_rows]))
+    rows = torch.unique(torch.cat([_sampled_rows(h[2], step=4099), long_rows]))
+    return dt, data, indices, indptr, shape, p, h, rows, long_rows
+
+
+def test_banded_precision_spmm_full_size(banded):
+    """Precision-form SpMM (N = 32) of the banded-plus-random config: float32
+    result, column checksum, sampled and long rows against FP64 of the same
+    half-precision inputs (long rows compensated: 2e-7)."""
+    dt, data, indices, indptr, shape, p, h, rows, long_rows = banded
+    B = synthetic.dense_operand(shape[1], 32, seed=1, dtype=dt, device=DEV)
+    C = fs.flagsparse_spmm_csr_mixed(B=B, prepared=p)
+    assert C.dtype == torch.float32
+    _colsum_check(C, data, indices, B, 3e-5)
     sd, si, sp = _sub_csr(*h, rows)
     ex, mag = orc.spmm_csr_exact(sd, si, sp, B.cpu())
     assert scaled_error(C.cpu()[rows], ex, mag) <= 3e-5
     lr = torch.isin(rows, long_rows)
     assert int(lr.sum()) > 0
     assert scaled_error(C.cpu()[rows][lr], ex[lr], mag[lr]) <= 2e-7
+
+
+def test_banded_precision_spmv_full_size(banded):
+    """Precision-form SpMV of the same config: float32 result, checksum
+    sum(y) = (1^T A) x, sampled and long rows against FP64 (long rows
+    compensated: 2e-7)."""
+    dt, data, indices, indptr, shape, p, h, rows, long_rows = banded
+    x = synthetic.dense_vector(shape[1], seed=3, dtype=dt, device=DEV)
+    y = fs.flagsparse_spmv_csr_mixed(x=x, prepared=p)
+    assert y.dtype == torch.float32
+    _colsum_check(y.unsqueeze(1), data, indices, x.unsqueeze(1), 3e-5)
+    sd, si, sp = _sub_csr(*h, rows)
+    ex, mag = orc.spmv_csr_exact(sd, si, sp, x.cpu())
+    assert scaled_error(y.cpu()[rows], ex, mag) <= 3e-5
+    lr = torch.isin(rows, long_rows)
+    assert scaled_error(y.cpu()[rows][lr], ex[lr], mag[lr]) <= 2e-7
 
 
 def test_bsr_tensor_core_full_size():

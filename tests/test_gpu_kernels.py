@@ -242,3 +242,77 @@ def test_gather_plan_rejects_unaligned_operands():
     with pytest.raises(ValueError, match="16-byte aligned"):
         _plan.run_spmm(data.to(DEV), indices.to(DEV), indptr.to(DEV), n_rows, n_cols, B, C, nat.ACC_NATIVE,
                        _plan.KernelPlan(nat.ALGO_GATHER, items_per_unit=16))
+
+
+def test_merge_runs_kernel_matches_oracle():
+    """fsb_merge_runs (binary searches) equals the oracle's linear walk."""
+    for pattern, items, snap in (("skewed", 128, 0), ("skewed", 77, 30), ("long_rows", 256, 64),
+                                 ("empty_rows", 4, 0), ("boundaries", 33, 0), ("all_empty", 8, 0)):
+        data, indices, indptr, (n_rows, n_cols) = csr_from_lengths(EDGE_LENGTHS[pattern], 20000, seed=29)
+        dptr = indptr.to(DEV)
+        plan = _plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=items, snap=snap)
+        plan.ensure_coords(dptr, n_rows, data.numel())
+        plan.ensure_runs(dptr, n_rows, 8)
+        ref = orc.merge_runs(indptr, n_rows, plan.coords.cpu())
+        assert torch.equal(plan.runs.cpu()[: ref.numel()], ref), (pattern, items, snap)
+
+
+def _spmm_two_kernel(d, n_rows, n_cols, B, C, acc, plan):
+    """The same SEQ plan with split rows finished by the separate fix-up
+    kernel (no unit runs in the C plan)."""
+    cm = nat.make_csr(d[0], d[1], d[2], n_rows, n_cols)
+    cp = nat.make_plan(plan.algo, items_per_unit=plan.items_per_unit, n_tile=plan.n_tile, coords=plan.coords,
+                       n_units=plan.n_units, comp_threshold=plan.comp_threshold, grid_blocks=plan.grid_blocks,
+                       flags=plan.flags)
+    out = nat.dtype_code(C.dtype)
+    ws, nbytes = _plan._workspace(True, cm, B.shape[1], acc, out, cp, B.device)
+    rc = nat.library().fsb_spmm_csr(cm, nat.ptr(B), int(B.stride(0)), int(B.shape[1]), nat.ptr(C), int(C.stride(0)),
+                                    out, int(acc), cp, nat.ptr(ws), nbytes, nat.stream_handle(B.device))
+    nat.check(rc, "fsb_spmm_csr (two-kernel)")
+
+
+SEQ_FINISH_PLANS = [(16, 0, 0, 0, 0), (100, 0, 0, 0, 0), (256, 128, 0, 0, 0), (2048, 0, 0, 0, 0),
+                    (128, 64, 32, 0, 0), (77, 0, 8, 0, 0), (16, 0, 0, 1, 0), (64, 0, 0, 3, 0),
+                    (128, 64, 0, 0, 0), (64, 64, 0, 2, 0)]
+
+
+@pytest.mark.parametrize("pattern", ["skewed", "long_rows", "boundaries", "empty_rows"])
+@pytest.mark.parametrize("n_dense", [1, 8, 64, 96])
+@pytest.mark.parametrize("mode", [SPMM_MODES[0], SPMM_MODES[1], SPMM_MODES[2], SPMM_MODES[5], SPMM_MODES[-1]],
+                         ids=_mode_id)
+def test_seq_in_kernel_finish_equals_fixup_kernel(pattern, n_dense, mode):
+    """Split rows finished inside k_spmm_seq (tickets, last unit sums in unit
+    order) equal the two-kernel form bit for bit, on two calls in a row, and
+    leave every ticket counter at zero."""
+    dtype, acc, out_dtype, _ = mode
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths(EDGE_LENGTHS[pattern], 13000, seed=31, dtype=dtype)
+    d = (data.to(DEV), indices.to(DEV), indptr.to(DEV))
+    Bd = dense((n_cols, n_dense), 32, dtype).to(DEV)
+    for items, snap, n_tile, grid, flags in SEQ_FINISH_PLANS:
+        plan = _plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=items, snap=snap, n_tile=n_tile, grid_blocks=grid,
+                                flags=flags)
+        ref = torch.full((n_rows, n_dense), float("nan"), dtype=out_dtype, device=DEV)
+        plan.ensure_coords(d[2], n_rows, data.numel())
+        _spmm_two_kernel(d, n_rows, n_cols, Bd, ref, acc, plan)
+        for _ in range(2):
+            C = torch.full((n_rows, n_dense), float("nan"), dtype=out_dtype, device=DEV)
+            _plan.run_spmm(*d, n_rows, n_cols, Bd, C, acc, plan)
+            assert torch.equal(C, ref), (pattern, n_dense, items, snap, n_tile, grid, flags)
+        assert plan.in_kernel_finish() and int(plan.tickets.abs().sum()) == 0
+
+
+def test_seq_in_kernel_finish_compensated_rows():
+    """Compensated (s, c) partials of long bf16 rows finish in the kernel with
+    the two-kernel form's bits."""
+    lengths = [8192] * 4 + [68] * 100 + [6000]
+    data, indices, indptr, (n_rows, n_cols) = csr_from_lengths(lengths, 12000, seed=33, dtype=torch.bfloat16)
+    d = (data.to(DEV), indices.to(DEV), indptr.to(DEV))
+    Bd = dense((n_cols, 32), 34, torch.bfloat16).to(DEV)
+    for items, snap in ((256, 64), (1024, 0), (97, 0)):
+        plan = _plan.KernelPlan(nat.ALGO_SEQ, items_per_unit=items, snap=snap, comp_threshold=4096)
+        plan.ensure_coords(d[2], n_rows, data.numel())
+        ref = torch.empty((n_rows, 32), dtype=torch.float32, device=DEV)
+        _spmm_two_kernel(d, n_rows, n_cols, Bd, ref, nat.ACC_COMP, plan)
+        C = torch.empty_like(ref)
+        _plan.run_spmm(*d, n_rows, n_cols, Bd, C, nat.ACC_COMP, plan)
+        assert torch.equal(C, ref), (items, snap)

@@ -31,7 +31,7 @@ def test_library_exports_every_declared_symbol():
 
 def test_abi_version_and_status_strings():
     lib = nat.library()
-    assert lib.fsb_abi_version() == 1
+    assert lib.fsb_abi_version() == 2
     assert lib.fsb_status_string(0) == b"ok"
     assert b"workspace" in lib.fsb_status_string(nat.FSB_ERR_WORKSPACE)
 
