@@ -600,9 +600,32 @@ class PrecisionBanded:
         }
 
     def plan_desc(self):
-        from flagsparse_public_b200.sparse_operations.precision import _mixed_plan
+        from flagsparse_public_b200.sparse_operations.precision import _mixed_plan, _structured_form
 
-        return _mixed_plan(self.half[torch.bfloat16][0], "spmm", self.n_dense).describe()
+        p = self.half[torch.bfloat16][0]
+        form = _structured_form(p)
+        if form is not None:
+            return {"kind": "structured", "band": "tcgen05 tiles of 128 rows (K-major runs x MN-major B span)",
+                    "long_rows": "tiles of 512 rows x 1024 columns streamed through shared memory"
+                    if form.lt_rec is not None else "chunks of 1024 nonzeros", **form.stats()}
+        return _mixed_plan(p, "spmm", self.n_dense).describe()
+
+    def roofline_note(self, out):
+        """The structured kernels read run values without indices and the long
+        rows as prepared records: the bytes they must move, and the roofline
+        fraction against them (the metric's useful bytes count int32 indices
+        for every nonzero)."""
+        from flagsparse_public_b200.sparse_operations.precision import _structured_form
+
+        p = self.half[torch.bfloat16][0]
+        form = _structured_form(p)
+        if form is None:
+            return {}
+        moved = form.moved_bytes(self.shape[0], self.shape[1], 2, p.kernel_indptr.element_size(), self.n_dense)
+        achieved = moved / (statistics.mean(out["times"]) * 1e-3) / 1e9
+        return {"moved_bytes": moved, "achieved_moved": achieved, "frac_moved": achieved / out["roofline"]["peak"],
+                "moved_what": "bytes the structured kernels must move (run values without indices, prepared "
+                              "long-row records, B and C once)"}
 
     def force_plan(self, plan):
         self.half[torch.bfloat16][0]._plans[("spmm", self.n_dense)] = plan

@@ -102,7 +102,9 @@ class FsbStruct(ctypes.Structure):
         ("lt_groups", ctypes.c_int64),
         ("lt_col_blocks", ctypes.c_int64),
         ("lt_rec_cap", ctypes.c_int32),
-        ("reserved2", ctypes.c_int32),
+        ("lt_rows", ctypes.c_int32),
+        ("lt_cols", ctypes.c_int32),
+        ("reserved3", ctypes.c_int32),
         ("lt_rec", ctypes.c_void_p),
         ("lt_seg_start", ctypes.c_void_p),
         ("lt_seg_len", ctypes.c_void_p),

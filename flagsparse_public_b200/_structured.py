@@ -24,8 +24,10 @@ from . import _native as nat
 from . import _plan
 
 LONG_MIN = 1024  # rows with more nonzeros take the long-row kernels
-LT_ROWS, LT_COLS, LT_RS = 512, 1024, 520  # SpMM long-row tiles: rows per group, columns per block, row starts
-LT_REC_CAP_MAX = 8192  # longest tile segment (records) the shared-memory stages take
+# SpMM long-row tiles: rows per group and columns per block (the compiled
+# shape, two shared-memory stages)
+LT_ROWS = 512
+LT_COLS = 1024
 MIN_RUN = 16  # shorter runs of consecutive columns count as none
 CHUNK_NNZ = 1024  # SpMM: nonzeros per chunk of a long row
 XBLOCK = 65536  # SpMV: columns of x per shared-memory block (128 KB of 16-bit values)
@@ -39,7 +41,7 @@ class StructuredForm:
 
     __slots__ = ("run_col", "run_off", "run_len", "tile_base", "tile_span", "max_span", "long_rows", "chunk_row",
                  "chunk_ptr", "seg_ptr", "seg_val", "seg_off", "n_long", "n_chunks", "xblock", "n_xblocks",
-                 "run_nnz", "long_nnz", "nnz", "lt_groups", "lt_col_blocks", "lt_rec_cap", "lt_rec", "lt_seg_start",
+                 "run_nnz", "long_nnz", "nnz", "lt_groups", "lt_col_blocks", "lt_rec_cap", "lt_rows", "lt_rec", "lt_seg_start",
                  "lt_seg_len", "lt_row_start", "_c", "_ws")
 
     def worthwhile(self):
@@ -48,6 +50,26 @@ class StructuredForm:
     def stats(self):
         return {"run_nnz": self.run_nnz, "long_nnz": self.long_nnz, "nnz": self.nnz, "long_rows": self.n_long,
                 "chunks": self.n_chunks, "max_span": self.max_span, "xblocks": self.n_xblocks}
+
+    def moved_bytes(self, n_rows, n_cols, value_bytes, ptr_bytes, n_dense=0):
+        """Algorithmic bytes of one structured product: run values without
+        indices, scattered nonzeros with their indices, per-row descriptors
+        (run column, offset, length) and row offsets, the long rows' prepared
+        stream (SpMM: 32-bit records and per-segment row starts; SpMV: values
+        and 16-bit offsets), the dense operand read once and the result
+        written once (SpMV: n_dense = 0)."""
+        short_scatter = self.nnz - self.run_nnz - self.long_nnz
+        b = self.run_nnz * value_bytes + short_scatter * (value_bytes + 4) + n_rows * (12 + ptr_bytes)
+        if n_dense:
+            if self.lt_rec is not None:
+                b += self.lt_rec.numel() * 4 + self.lt_row_start.numel() * 2 + self.lt_seg_start.numel() * 12
+            else:
+                b += self.long_nnz * (value_bytes + 4)
+            b += n_cols * n_dense * value_bytes + n_rows * n_dense * 4
+        else:
+            b += self.long_nnz * (value_bytes + 2) + (self.n_xblocks * self.n_long + 1) * 8
+            b += n_cols * value_bytes + n_rows * 4
+        return int(b)
 
     def c_struct(self):
         if self._c is None:
@@ -66,6 +88,7 @@ class StructuredForm:
             s.seg_off = self.seg_off.data_ptr() if self.n_long and self.seg_off.numel() else 0
             if self.lt_rec is not None:
                 s.lt_groups, s.lt_col_blocks, s.lt_rec_cap = self.lt_groups, self.lt_col_blocks, self.lt_rec_cap
+                s.lt_rows, s.lt_cols = self.lt_rows, LT_COLS
                 s.lt_rec = self.lt_rec.data_ptr()
                 s.lt_seg_start = self.lt_seg_start.data_ptr()
                 s.lt_seg_len = self.lt_seg_len.data_ptr()
@@ -116,7 +139,7 @@ def build(data, indices, indptr, n_rows, n_cols):
     f.n_xblocks = max(1, -(-n_cols // f.xblock))
     f.n_chunks = 0
     f.chunk_row = f.chunk_ptr = f.seg_ptr = f.seg_val = f.seg_off = None
-    f.lt_groups = f.lt_col_blocks = f.lt_rec_cap = 0
+    f.lt_groups = f.lt_col_blocks = f.lt_rec_cap = f.lt_rows = 0
     f.lt_rec = f.lt_seg_start = f.lt_seg_len = f.lt_row_start = None
     if f.n_long:
         # SpMM: chunks of CHUNK_NNZ nonzeros, chunk_ptr[l] = first chunk of long row l
@@ -149,40 +172,48 @@ def build(data, indices, indptr, n_rows, n_cols):
     return f
 
 
+def _lt_rec_cap_max(rows, cols, n_dense_max=32):
+    """Longest segment (records) whose stages fit in shared memory."""
+    stages = 2
+    budget = (227 * 1024 - 2048) // stages - cols * n_dense_max * 2 - (rows + 8) * 2
+    return max(0, budget // 16 * 4)
+
+
 def _build_long_tiles(f, data, gidx, lpos, cols, n_cols):
     """SpMM: the long rows' nonzeros as (row group of LT_ROWS, column block
     of LT_COLS) segments of 32-bit records (value bits | column inside the
     block << 16), ordered by row (each row's columns in order: stable sort),
-    padded to 4 records, with LT_RS 16-bit per-row record starts per segment.
-    Left out (SpMM runs the long rows in chunks) when a segment is longer
-    than LT_REC_CAP_MAX records."""
+    padded to 4 records, with LT_ROWS + 8 16-bit per-row record starts per
+    segment.  Left out (SpMM runs the long rows in chunks) when a segment is
+    longer than the shared-memory stages take."""
     dev = data.device
-    groups = -(-f.n_long // LT_ROWS)
+    rows_g, rs_n = LT_ROWS, LT_ROWS + 8
+    groups = -(-f.n_long // rows_g)
     blocks = max(1, -(-n_cols // LT_COLS))
     n_seg = groups * blocks
-    key = ((lpos // LT_ROWS) * blocks + cols // LT_COLS) * LT_ROWS + lpos % LT_ROWS
-    skey, perm = _plan.stable_sort(key, key_bound=n_seg * LT_ROWS)
-    offs = _plan.sorted_keys_to_offsets(skey, n_seg * LT_ROWS)  # [n_seg * LT_ROWS + 1]
-    first = offs[::LT_ROWS]  # segment boundaries, n_seg + 1 entries
+    key = ((lpos // rows_g) * blocks + cols // LT_COLS) * rows_g + lpos % rows_g
+    skey, perm = _plan.stable_sort(key, key_bound=n_seg * rows_g)
+    offs = _plan.sorted_keys_to_offsets(skey, n_seg * rows_g)  # [n_seg * rows_g + 1]
+    first = offs[::rows_g]  # segment boundaries, n_seg + 1 entries
     cnt = first[1:] - first[:-1]
     seg_len = (cnt + 3) // 4 * 4
     cap = int(seg_len.max())
-    if cap > LT_REC_CAP_MAX:
+    if cap > _lt_rec_cap_max(rows_g, LT_COLS):
         return
     seg_start = torch.zeros(n_seg, dtype=torch.int64, device=dev)
     seg_start[1:] = torch.cumsum(seg_len, 0)[:-1]
     total_pad = int(seg_len.sum())
-    grid = torch.arange(n_seg, device=dev)[:, None] * LT_ROWS + torch.arange(LT_ROWS + 1, device=dev)[None, :]
+    grid = torch.arange(n_seg, device=dev)[:, None] * rows_g + torch.arange(rows_g + 1, device=dev)[None, :]
     rs = offs[grid] - first[:-1][:, None]
-    row_start = torch.empty((n_seg, LT_RS), dtype=torch.int64, device=dev)
-    row_start[:, : LT_ROWS + 1] = rs
-    row_start[:, LT_ROWS + 1:] = rs[:, LT_ROWS:]
-    seg_of = skey // LT_ROWS
+    row_start = torch.empty((n_seg, rs_n), dtype=torch.int64, device=dev)
+    row_start[:, : rows_g + 1] = rs
+    row_start[:, rows_g + 1:] = rs[:, rows_g:]
+    seg_of = skey // rows_g
     pos = seg_start[seg_of] + (torch.arange(skey.numel(), device=dev) - first[:-1][seg_of])
     vbits = data[gidx[perm]].view(torch.int16).to(torch.int32) & 0xFFFF
     rec = torch.zeros(max(total_pad, 4), dtype=torch.int32, device=dev)
     rec[pos] = vbits | ((cols[perm] % LT_COLS).to(torch.int32) << 16)
-    f.lt_groups, f.lt_col_blocks, f.lt_rec_cap = groups, blocks, cap
+    f.lt_groups, f.lt_col_blocks, f.lt_rec_cap, f.lt_rows = groups, blocks, cap, rows_g
     f.lt_rec = rec
     f.lt_seg_start = seg_start
     f.lt_seg_len = seg_len.to(torch.int32)

@@ -604,6 +604,13 @@ __host__ __device__ constexpr uint32_t band_idesc() {
 template <int X>
 __device__ __forceinline__ void tmem_ld(uint32_t taddr, uint32_t* d);
 template <>
+__device__ __forceinline__ void tmem_ld<8>(uint32_t taddr, uint32_t* d) {
+    asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+                 : "=r"(d[0]), "=r"(d[1]), "=r"(d[2]), "=r"(d[3]), "=r"(d[4]), "=r"(d[5]), "=r"(d[6]), "=r"(d[7])
+                 : "r"(taddr)
+                 : "memory");
+}
+template <>
 __device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, uint32_t* d) {
     asm volatile(
         "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
@@ -614,24 +621,27 @@ __device__ __forceinline__ void tmem_ld<16>(uint32_t taddr, uint32_t* d) {
         : "memory");
 }
 
-// Band tiles on the tensor cores.  One CTA of 128 threads per tile of 128
-// rows; thread i owns row i of the tile: its descriptors, its run, its TMEM
-// lane, its scattered nonzeros and its C row.
+// Band tiles on the tensor cores.  One CTA of 256 threads per tile of 128
+// rows; threads t and t + 128 share row t % 128 (its descriptors and
+// scattered nonzeros), each owning half of the row's N columns in the
+// epilogue: warp w reads TMEM lane quarter w % 4, columns (w / 4) * N / 2 on.
 //   A (dynamic shared memory, K-major SWIZZLE_NONE core matrices): element
 //     (m, k) at (m / 8) * sbo_a + (k / 8) * 128 + (m % 8) * 16 + (k % 8) * 2,
 //     sbo_a = span / 8 * 128; row m holds its run at k = run_col - base, zeros
-//     elsewhere.  Thread m reads its run as the 16-byte aligned chunks holding
-//     it (up to kRunChunks per round, all in flight together) and stores the
-//     run's elements one by one.
+//     elsewhere.  The row's two threads read its run as the 16-byte aligned
+//     chunks holding it (even / odd chunks, all in flight together) and store
+//     the run's elements one by one.
 //   B (MN-major core matrices, after A): element (k, n) at (k / 8) * lbo_b +
 //     (n / 8) * 128 + (k % 8) * 16 + (n % 8) * 2, lbo_b = N / 8 * 128; the
 //     span's B rows with 16-byte loads, four per thread in flight.
 // The first kPrefetch scattered nonzeros of each row: indices with the run,
-// B rows while the MMAs run.  span / 16 MMAs of 128 x N x 16 are issued by one
-// thread and committed to an mbarrier (bounded wait).  Long rows are left to
-// the long-row kernels.
+// the thread's half B rows while the MMAs run.  span / 16 MMAs of 128 x N x 16
+// are issued by one thread and committed to an mbarrier (bounded wait).  Long
+// rows are left to the long-row kernels.
+constexpr int kBandThreads = 256;
+
 template <class V, class I, class P, int N>
-__global__ void __launch_bounds__(kThreads)
+__global__ void __launch_bounds__(kBandThreads)
 k_struct_spmm_band(const V* __restrict__ val, const I* __restrict__ col, const P* __restrict__ ptr, int64_t n_rows,
                    int64_t n_cols, const int32_t* __restrict__ run_col, const int32_t* __restrict__ run_off,
                    const int32_t* __restrict__ run_len, const int64_t* __restrict__ tile_base,
@@ -641,19 +651,22 @@ k_struct_spmm_band(const V* __restrict__ val, const I* __restrict__ col, const P
     constexpr bool kBf16 = std::is_same<V, __nv_bfloat16>::value;
     constexpr int kTmemCols = N <= 32 ? 32 : 64;
     constexpr uint32_t kLboB = (N / 8) * 128;
-    constexpr int kCh = N / 8;  // 16-byte chunks per B row
-    constexpr int kVec = 8;     // 16-bit values per 16-byte chunk
-    constexpr int kRunChunks = 10;
+    constexpr int kCh = N / 8;    // 16-byte chunks per B row
+    constexpr int kHalf = N / 2;  // columns per thread in the epilogue
+    constexpr int kHCh = kCh / 2;
+    constexpr int kVec = 8;       // 16-bit values per 16-byte chunk
+    constexpr int kRunChunks = 5;
     constexpr int kPrefetch = N <= 32 ? 4 : 2;
     extern __shared__ __align__(1024) unsigned char sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, warp = tid >> 5;
+    const int row_t = tid & (kTileRows - 1), half = tid >> 7;
     const int64_t t = blockIdx.x, r0 = t * kTileRows;
     // descriptors of this thread's row and of the tile
     const int64_t kbase = tile_base[t];
     const int span = tile_span[t];
-    const int64_t r = r0 + tid;
+    const int64_t r = r0 + row_t;
     const int rl = r < n_rows ? run_len[r] : -1;
     int64_t s = 0, e = 0;
     int ro = 0, kc = 0;
@@ -694,7 +707,7 @@ k_struct_spmm_band(const V* __restrict__ val, const I* __restrict__ col, const P
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    for (int i = tid; i < kTileRows * span * 2 / 16; i += kThreads)
+    for (int i = tid; i < kTileRows * span * 2 / 16; i += kBandThreads)
         reinterpret_cast<uint4*>(sa)[i] = make_uint4(0, 0, 0, 0);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
@@ -704,11 +717,11 @@ k_struct_spmm_band(const V* __restrict__ val, const I* __restrict__ col, const P
     if (span > 0) {
         // the span's B rows -> B, four 16-byte loads in flight per thread
         const int n_q = span * kCh;
-        for (int i0 = tid; i0 < n_q; i0 += 4 * kThreads) {
+        for (int i0 = tid; i0 < n_q; i0 += 4 * kBandThreads) {
             uint4 q[4];
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const int i = i0 + u * kThreads;
+                const int i = i0 + u * kBandThreads;
                 q[u] = make_uint4(0, 0, 0, 0);
                 if (i < n_q) {
                     const int64_t br = kbase + i / kCh;
@@ -717,32 +730,33 @@ k_struct_spmm_band(const V* __restrict__ val, const I* __restrict__ col, const P
             }
 #pragma unroll
             for (int u = 0; u < 4; ++u) {
-                const int i = i0 + u * kThreads;
+                const int i = i0 + u * kBandThreads;
                 if (i < n_q) {
                     const int k = i / kCh, ch = i % kCh;
                     *reinterpret_cast<uint4*>(sb + (k >> 3) * kLboB + ch * 128 + (k & 7) * 16) = q[u];
                 }
             }
         }
-        // this thread's run -> row tid of A: the aligned chunks holding it
-        // (an aligned chunk holding a valid element lies inside one page)
+        // the row's run -> row row_t of A: the aligned chunks holding it
+        // (even chunks by the first thread, odd by the second; an aligned
+        // chunk holding a valid element lies inside one page)
         if (rn > 0) {
             const uintptr_t a0 = reinterpret_cast<uintptr_t>(val + s + ro);
             const V* cbase = reinterpret_cast<const V*>(a0 & ~(uintptr_t)15);
             const int lead = (int)((a0 & 15u) / sizeof(V));
             const int n_ch = (lead + rn + kVec - 1) / kVec;
-            const uint32_t row_off = (uint32_t)(tid >> 3) * sbo_a + (uint32_t)(tid & 7) * 16;
-            for (int c0 = 0; c0 < n_ch; c0 += kRunChunks) {
+            const uint32_t row_off = (uint32_t)(row_t >> 3) * sbo_a + (uint32_t)(row_t & 7) * 16;
+            for (int c0 = half; c0 < n_ch; c0 += 2 * kRunChunks) {
                 vec_t<V, kVec> w[kRunChunks];
 #pragma unroll
                 for (int u = 0; u < kRunChunks; ++u)
-                    if (c0 + u < n_ch) w[u] = ld_stream<V, kVec>(cbase + (c0 + u) * kVec);
+                    if (c0 + 2 * u < n_ch) w[u] = ld_stream<V, kVec>(cbase + (c0 + 2 * u) * kVec);
 #pragma unroll
                 for (int u = 0; u < kRunChunks; ++u) {
-                    if (c0 + u < n_ch) {
+                    if (c0 + 2 * u < n_ch) {
 #pragma unroll
                         for (int z = 0; z < kVec; ++z) {
-                            const int q = (c0 + u) * kVec + z - lead;
+                            const int q = (c0 + 2 * u) * kVec + z - lead;
                             if (q >= 0 && q < rn) {
                                 const int k = kc + q;
                                 *reinterpret_cast<V*>(sa + row_off + (uint32_t)(k >> 3) * 128 + (uint32_t)(k & 7) * 2) =
@@ -775,13 +789,13 @@ k_struct_spmm_band(const V* __restrict__ val, const I* __restrict__ col, const P
                          smem_u32(&bar))
                      : "memory");
     }
-    // the prefetched scattered nonzeros' B rows while the MMAs run
-    uint4 qp[kPrefetch][kCh];
+    // this thread's half of the prefetched scattered B rows while the MMAs run
+    uint4 qp[kPrefetch][kHCh];
 #pragma unroll
     for (int u = 0; u < kPrefetch; ++u)
 #pragma unroll
-        for (int ch = 0; ch < kCh; ++ch)
-            qp[u][ch] = u < n_sc ? __ldg(reinterpret_cast<const uint4*>(B + idx(cp[u]) * ldb + ch * 8))
+        for (int ch = 0; ch < kHCh; ++ch)
+            qp[u][ch] = u < n_sc ? __ldg(reinterpret_cast<const uint4*>(B + idx(cp[u]) * ldb + half * kHalf + ch * 8))
                                  : make_uint4(0, 0, 0, 0);
     bool ok = true;
     if (span > 0) {
@@ -789,22 +803,23 @@ k_struct_spmm_band(const V* __restrict__ val, const I* __restrict__ col, const P
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         if (!ok && tid == 0) atomicExch(err, FSB_ERR_TIMEOUT);
     }
-    float acc[N];
+    float acc[kHalf];
     if (span > 0 && ok) {
-        uint32_t d[N];
+        uint32_t d[kHalf];
 #pragma unroll
-        for (int q = 0; q < N / 16; ++q) tmem_ld<16>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)q * 16, d + q * 16);
+        for (int q = 0; q < kHalf / 8; ++q)
+            tmem_ld<8>(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(half * kHalf + q * 8), d + q * 8);
         asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
-        for (int n = 0; n < N; ++n) acc[n] = __uint_as_float(d[n]);
+        for (int n = 0; n < kHalf; ++n) acc[n] = __uint_as_float(d[n]);
     } else {
 #pragma unroll
-        for (int n = 0; n < N; ++n) acc[n] = 0.f;
+        for (int n = 0; n < kHalf; ++n) acc[n] = 0.f;
     }
     if (ok && rl >= 0) {
-        auto fma_row = [&](float a, const uint4 (&q)[kCh]) {
+        auto fma_row = [&](float a, const uint4 (&q)[kHCh]) {
 #pragma unroll
-            for (int ch = 0; ch < kCh; ++ch) {
+            for (int ch = 0; ch < kHCh; ++ch) {
                 V b8[8];
                 memcpy(b8, &q[ch], 16);
 #pragma unroll
@@ -818,20 +833,20 @@ k_struct_spmm_band(const V* __restrict__ val, const I* __restrict__ col, const P
             const int64_t ka = q < ro ? s + q : s + q + rn;
             const bool two = q + 1 < n_sc;
             const int64_t kb = two ? ((q + 1) < ro ? s + q + 1 : s + q + 1 + rn) : ka;
-            const V* ba = B + idx(ld_stream1(col + ka)) * ldb;
-            const V* bb = B + idx(ld_stream1(col + kb)) * ldb;
-            uint4 qa[kCh], qb[kCh];
+            const V* ba = B + idx(ld_stream1(col + ka)) * ldb + half * kHalf;
+            const V* bb = B + idx(ld_stream1(col + kb)) * ldb + half * kHalf;
+            uint4 qa[kHCh], qb[kHCh];
 #pragma unroll
-            for (int ch = 0; ch < kCh; ++ch) {
+            for (int ch = 0; ch < kHCh; ++ch) {
                 qa[ch] = __ldg(reinterpret_cast<const uint4*>(ba + ch * 8));
                 qb[ch] = __ldg(reinterpret_cast<const uint4*>(bb + ch * 8));
             }
             fma_row(to_f32(ld_stream1(val + ka)), qa);
             if (two) fma_row(to_f32(ld_stream1(val + kb)), qb);
         }
-        float* dst = C + r * ldc;
+        float* dst = C + r * ldc + half * kHalf;
 #pragma unroll
-        for (int n = 0; n < N; n += 4)
+        for (int n = 0; n < kHalf; n += 4)
             __stcs(reinterpret_cast<float4*>(dst + n), make_float4(acc[n], acc[n + 1], acc[n + 2], acc[n + 3]));
     }
     if (!ok) {
@@ -886,15 +901,17 @@ int check_struct(const fsb_csr* A, const fsb_struct* S, const char* who) {
 }
 
 // The tiled long-row kernel runs when the structure carries its record
-// stream, the dense width is 16 or 32, B rows are contiguous (ldb == n_dense)
-// and two stages fit in shared memory.
+// stream in the compiled tile shape (lt_rows 512, lt_cols 1024), the dense
+// width is 16 or 32, B rows are contiguous (ldb == n_dense) and two stages fit
+// in shared memory.
 int64_t lt_stage_bytes(const fsb_struct* S, int64_t n_dense) {
     return (int64_t)kLtCols * n_dense * 2 + kLtRsEntries * 2 + (int64_t)S->lt_rec_cap * 4;
 }
 bool lt_usable(const fsb_struct* S, int64_t n_dense, int64_t ldb) {
-    return S->lt_rec && S->lt_seg_start && S->lt_seg_len && S->lt_row_start && S->lt_groups > 0 &&
-           S->lt_col_blocks > 0 && S->lt_rec_cap >= 0 && S->lt_rec_cap % 4 == 0 && (n_dense == 16 || n_dense == 32) &&
-           ldb == n_dense && 2 * lt_stage_bytes(S, n_dense) <= 227 * 1024 - 2048;
+    return S->lt_rows == kLtRows && S->lt_cols == kLtCols && S->lt_rec && S->lt_seg_start && S->lt_seg_len &&
+           S->lt_row_start && S->lt_groups > 0 && S->lt_col_blocks > 0 && S->lt_rec_cap >= 0 &&
+           S->lt_rec_cap % 4 == 0 && (n_dense == 16 || n_dense == 32) && ldb == n_dense &&
+           2 * lt_stage_bytes(S, n_dense) <= 227 * 1024 - 2048;
 }
 // Column ranges per row group: about one CTA per SM in all.
 int64_t lt_ranges(const fsb_struct* S) {
@@ -1067,7 +1084,7 @@ extern "C" int fsb_struct_spmm(const fsb_csr* A, const fsb_struct* S, const void
                 auto band = [&](auto kern) -> int {
                     if (smem > 48 * 1024)
                         cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-                    kern<<<(unsigned)n_tiles, kThreads, smem, st>>>(val, col, ptr, A->n_rows, A->n_cols, S->run_col,
+                    kern<<<(unsigned)n_tiles, kBandThreads, smem, st>>>(val, col, ptr, A->n_rows, A->n_cols, S->run_col,
                                                                     S->run_off, S->run_len, S->tile_base,
                                                                     S->tile_span, Bv, ldb, C, ldc, err);
                     return fsb_host::check_launch("k_struct_spmm_band");

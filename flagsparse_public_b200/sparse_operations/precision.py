@@ -118,6 +118,9 @@ def _resolve(data, indices, indptr, shape, prepared, compensate_above, layout="a
     if prepared is None:
         if any(a is None for a in (data, indices, indptr, shape)):
             raise ValueError("data, indices, indptr, and shape are required when prepared is not provided")
+        # a one-shot call runs one product: building the structured form costs
+        # more than it saves, so "auto" keeps the CSR kernels here
+        layout = "csr" if layout == "auto" else layout
         prepared = prepare_csr_mixed(data, indices, indptr, shape, compensate_above=compensate_above, layout=layout)
     elif not isinstance(prepared, PreparedCsrMixed):
         raise TypeError("prepared must be a PreparedCsrMixed instance")

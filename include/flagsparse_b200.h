@@ -289,19 +289,22 @@ typedef struct fsb_struct {
                                  long row) segments of the regrouped nonzeros */
     const void* seg_val;      /* values of the long rows, by (block, row)     */
     const uint16_t* seg_off;  /* their columns minus the block's first column */
-    /* SpMM, optional (lt_rec null: chunks): the long rows in tiles of 512
-     * rows x 1024 columns.  Per (row group, column block) segment: records
-     * (value bits | column inside the block << 16), ordered by row, padded
-     * to a multiple of 4, starting at lt_seg_start (a multiple of 4), with
-     * 520 16-bit per-row record starts (513 used).                          */
-    int64_t lt_groups;          /* ceil(n_long / 512)                        */
-    int64_t lt_col_blocks;      /* ceil(n_cols / 1024)                       */
+    /* SpMM, optional (lt_rec null: chunks): the long rows in tiles of
+     * lt_rows rows x lt_cols columns (compiled: 512 x 1024).
+     * Per (row group, column block) segment: records (value bits | column
+     * inside the block << 16), ordered by row, padded to a multiple of 4,
+     * starting at lt_seg_start (a multiple of 4), with lt_rows + 8 16-bit
+     * per-row record starts (lt_rows + 1 used).                             */
+    int64_t lt_groups;          /* ceil(n_long / lt_rows)                    */
+    int64_t lt_col_blocks;      /* ceil(n_cols / lt_cols)                    */
     int32_t lt_rec_cap;         /* longest padded segment, in records        */
-    int32_t reserved2;
+    int32_t lt_rows;
+    int32_t lt_cols;
+    int32_t reserved3;
     const uint32_t* lt_rec;
     const int64_t* lt_seg_start; /* [lt_groups * lt_col_blocks]              */
     const int32_t* lt_seg_len;   /* [lt_groups * lt_col_blocks] padded        */
-    const uint16_t* lt_row_start;/* [lt_groups * lt_col_blocks * 520]         */
+    const uint16_t* lt_row_start;/* [lt_groups * lt_col_blocks * (lt_rows + 8)] */
 } fsb_struct;
 
 /* Per-row descriptors: the longest run of consecutive columns of each row of
