@@ -458,19 +458,84 @@ class SpmvPoisson:
         self.prepared._plans[("opt", 0)] = plan
         self.graph = self._capture(use_opt=True)
 
+    e2e_what = ("per step: the step's A (values, column indices, row offsets) and x, packed in one pinned host "
+                "buffer, -> device in one copy; the one-shot flagsparse_spmv_csr on them (structural check, its "
+                "device->host read, plan, product in one native call); y -> pinned host.  Steps back to back on "
+                "one stream (a look-ahead upload on a second stream measured slower: copies and the call's "
+                "check contend)")
+
     def host_inputs(self):
         data, indices, indptr = self.A
-        self.h = [t.cpu().pin_memory() for t in (data, indices, indptr, self.x)]
+        parts = [t.cpu() for t in (data, indices, indptr, self.x)]
+        self._layout, off = [], 0
+        for t in parts:
+            nb = t.numel() * t.element_size()
+            self._layout.append((off, nb, t.dtype))
+            off += (nb + 15) // 16 * 16  # 16-byte aligned sections
+        self.h_pack = torch.zeros(off, dtype=torch.uint8).pin_memory()
+        for (o, nb, _dt), t in zip(self._layout, parts):
+            self.h_pack[o:o + nb].copy_(t.view(torch.uint8))
         self.h_out = torch.empty(self.y.shape, dtype=self.y.dtype).pin_memory()
-        self.h2d_bytes = sum(t.numel() * t.element_size() for t in self.h)
+        self.h2d_bytes = off
         self.d2h_bytes = self.h_out.numel() * self.h_out.element_size()
 
     def e2e_step(self, device):
         import flagsparse_public_b200 as fs
 
-        d = [t.to(device, non_blocking=True) for t in self.h]
+        buf = self.h_pack.to(device, non_blocking=True)
+        d = [buf[o:o + nb].view(dt) for o, nb, dt in self._layout]
         y = fs.flagsparse_spmv_csr(d[0], d[1], d[2], d[3], self.shape, use_opt=True)
         self.h_out.copy_(y, non_blocking=True)
+
+    def e2e_check(self):
+        """The last downloaded result equals the resident one-shot product."""
+        import flagsparse_public_b200 as fs
+
+        ref = fs.flagsparse_spmv_csr(*self.A, self.x, self.shape, use_opt=True)
+        torch.cuda.synchronize()
+        if not torch.equal(self.h_out, ref.cpu()):
+            raise RuntimeError("end-to-end result differs from the resident product")
+
+    def e2e_breakdown(self, device):
+        """Each part of one step alone (us): the packed upload and the result
+        download (CUDA events), the one-shot call on resident inputs (host
+        wall time: check, read, plan, launch, product) and the product kernel
+        (CUDA-graph time per SpMV)."""
+        import time
+
+        import flagsparse_public_b200 as fs
+
+        def ev(fn, n=50):
+            for _ in range(3):
+                fn()
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            for _ in range(n):
+                fn()
+            e.record()
+            torch.cuda.synchronize()
+            return s.elapsed_time(e) * 1e3 / n
+
+        dbuf = torch.empty(self.h_pack.shape, dtype=torch.uint8, device=device)
+        up = ev(lambda: dbuf.copy_(self.h_pack, non_blocking=True))
+        down = ev(lambda: self.h_out.copy_(self.y, non_blocking=True))
+        data, indices, indptr = self.A
+
+        def call():
+            fs.flagsparse_spmv_csr(data, indices, indptr, self.x, self.shape, use_opt=True)
+
+        for _ in range(5):
+            call()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(50):
+            call()
+        torch.cuda.synchronize()
+        call_us = (time.perf_counter() - t0) * 1e6 / 50
+        kern = ev(self.step, 5) / self.graph_iters
+        return {"upload_us": round(up, 2), "oneshot_call_us": round(call_us, 2), "kernel_us": round(kern, 3),
+                "download_us": round(down, 2)}
 
     def fp64_error(self):
         from oracle import oracle as orc
@@ -1196,10 +1261,14 @@ def _e2e(wl, device, steps, warmup, world):
     if check is not None:
         check()
     per_step_bytes = wl.useful_bytes / getattr(wl, "graph_iters", 1)
-    return {"value": per_step_bytes * world / (e_ms * 1e-3) / 1e9, "unit": wl.unit, "ms_per_step": e_ms,
-            "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes,
-            "what": getattr(wl, "e2e_what", "pinned host A and dense operand -> device, public one-shot API "
-                                            "(prepare + product), result -> pinned host")}
+    out = {"value": per_step_bytes * world / (e_ms * 1e-3) / 1e9, "unit": wl.unit, "ms_per_step": e_ms,
+           "h2d_bytes_per_step": wl.h2d_bytes, "d2h_bytes_per_step": wl.d2h_bytes,
+           "what": getattr(wl, "e2e_what", "pinned host A and dense operand -> device, public one-shot API "
+                                           "(prepare + product), result -> pinned host")}
+    breakdown = getattr(wl, "e2e_breakdown", None)
+    if breakdown is not None:
+        out["breakdown"] = breakdown(device)
+    return out
 
 
 def measure(wl, name, args, device, flush, world, rank, steps, warmup, cpu_seconds, with_e2e=True):

@@ -28,6 +28,7 @@ FSB_F16, FSB_BF16, FSB_F32, FSB_F64, FSB_C64, FSB_C128, FSB_I32, FSB_I64 = range
 ACC_NATIVE, ACC_WIDE, ACC_COMP = 0, 1, 2
 ALGO_ROWS, ALGO_MERGE, ALGO_FLAT, ALGO_GATHER, ALGO_SEQ = 0, 1, 2, 3, 4
 PLAN_TMA_GATHER = 1  # fsb_plan.flags: SEQ with B rows staged by TMA tile::gather4
+PLAN_OVERLAP_LAUNCH = 2  # fsb_plan.flags: ROWS SpMV with programmatic dependent launch
 BSR_STAGE_TMA, BSR_STAGE_THREADS = 0, 1
 
 _DTYPE_CODES = {
@@ -128,6 +129,12 @@ _SIGNATURES = {
         [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_int64, ctypes.c_int32, ctypes.c_int64,
          ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
     ),
+    "fsb_csr_check_workspace_bytes": (ctypes.c_int64, [ctypes.c_int64, ctypes.c_int64]),
+    "fsb_csr_check": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
+    ),
     "fsb_merge_runs": (
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p,
@@ -137,6 +144,12 @@ _SIGNATURES = {
         ctypes.c_int,
         [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int,
          ctypes.POINTER(FsbPlan), ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p],
+    ),
+    "fsb_spmv_csr_checked_workspace_bytes": (ctypes.c_int64, [ctypes.POINTER(FsbCsr), ctypes.c_int, ctypes.c_int]),
+    "fsb_spmv_csr_checked": (
+        ctypes.c_int,
+        [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
+         ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(FsbPlan), ctypes.c_void_p],
     ),
     "fsb_spmv_csr_noalloc": (
         ctypes.c_int,
@@ -296,11 +309,38 @@ def check(status, what):
 
 
 def stream_handle(device):
-    return ctypes.c_void_p(torch.cuda.current_stream(device).cuda_stream)
+    """torch's current stream on ``device`` as a cudaStream_t."""
+    idx = device.index if isinstance(device, torch.device) else device
+    if idx is None:
+        idx = torch.cuda.current_device()
+    return ctypes.c_void_p(torch._C._cuda_getCurrentRawStream(idx))
 
 
 def ptr(t):
     return ctypes.c_void_p(t.data_ptr()) if t is not None and t.numel() > 0 else ctypes.c_void_p(0)
+
+
+_figures = threading.local()
+
+
+def csr_check(row_ptr, col_idx, n_rows):
+    """The eight structural figures of fsb_csr_check (row_ptr[0],
+    row_ptr[n_rows], rows of negative length, negative column indices, largest
+    column index, longest row, sum of squared row lengths, empty rows),
+    written by its kernels into a pinned buffer of this thread and read after
+    one stream synchronisation."""
+    buf = getattr(_figures, "buf", None)
+    if buf is None:
+        buf = _figures.buf = torch.empty(8, dtype=torch.int64).pin_memory()
+    n_rows, nnz = int(n_rows), int(col_idx.numel())
+    lib = library()
+    nbytes = int(lib.fsb_csr_check_workspace_bytes(n_rows, nnz))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=row_ptr.device)
+    rc = lib.fsb_csr_check(ptr(row_ptr), dtype_code(row_ptr.dtype), n_rows, ptr(col_idx), dtype_code(col_idx.dtype),
+                           nnz, ctypes.c_void_p(buf.data_ptr()), ptr(ws), nbytes, stream_handle(row_ptr.device))
+    check(rc, "fsb_csr_check")
+    torch.cuda.current_stream(row_ptr.device).synchronize()
+    return buf.tolist()
 
 
 def make_csr(values, col_idx, row_ptr, n_rows, n_cols, row_map=None):

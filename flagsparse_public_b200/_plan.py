@@ -202,7 +202,7 @@ def _pow2_clamp(v, lo, hi):
 
 
 def _vec_elems(dtype):
-    return max(1, 16 // (torch.empty((), dtype=dtype).element_size()))
+    return max(1, 16 // dtype.itemsize)
 
 
 def default_spmv_plan(stats, dtype, row_cap=0):
@@ -216,10 +216,10 @@ def default_spmv_plan(stats, dtype, row_cap=0):
         return KernelPlan(nat.ALGO_ROWS, lanes=lanes, row_cap=row_cap)
     skewed = stats.max_row > 8 * max(stats.mean_row, 1.0) + 256
     if skewed and stats.mean_row < 32:
-        ipt = 8 if torch.empty((), dtype=dtype).element_size() <= 4 else 4
+        ipt = 8 if dtype.itemsize <= 4 else 4
         return KernelPlan(nat.ALGO_MERGE, items_per_unit=SPMV_MERGE_THREADS * ipt)
     lanes = _pow2_clamp(2 * stats.mean_row / _vec_elems(dtype), 2, 32)
-    return KernelPlan(nat.ALGO_ROWS, lanes=lanes)
+    return KernelPlan(nat.ALGO_ROWS, lanes=lanes, flags=nat.PLAN_OVERLAP_LAUNCH)
 
 
 SM_COUNT = 148  # B200

@@ -52,6 +52,96 @@ __global__ void k_spmm_coo_atomic(const V* __restrict__ val, const I* __restrict
     }
 }
 
+// Structural check of a CSR matrix: row lengths from adjacent row offsets
+// and column indices in grid-stride loops, each CTA's six figures reduced in
+// shared memory and written to its slot of part[]; one CTA then folds the
+// slots into out[].  No memset or copy-engine work, and out[] may be pinned
+// host memory, so the check does not queue behind host<->device copies.
+constexpr int kCheckThreads = 256;
+constexpr int64_t kCheckMaxBlocks = 148 * 8;
+
+__device__ __forceinline__ unsigned long long check_fold(int f, unsigned long long a, unsigned long long b) {
+    return (f == 2 || f == 3) ? (a > b ? a : b) : a + b;  // slots 2, 3 are maxima
+}
+
+template <class P, class I>
+__global__ void __launch_bounds__(kCheckThreads) k_csr_check_part(const P* __restrict__ ptr, int64_t n_rows,
+                                                                   const I* __restrict__ col, int64_t nnz,
+                                                                   unsigned long long* __restrict__ part) {
+    // slot f of a CTA: rows of negative length, negative columns, largest
+    // column, longest row, sum of squared lengths, empty rows
+    unsigned long long v[6] = {0, 0, 0, 0, 0, 0};
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t t0 = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    for (int64_t r = t0; r < n_rows; r += stride) {
+        const int64_t len = idx(ptr[r + 1]) - idx(ptr[r]);
+        if (len < 0) {
+            ++v[0];
+        } else {
+            const unsigned long long u = (unsigned long long)len;
+            v[3] = u > v[3] ? u : v[3];
+            v[4] += u * u;
+            v[5] += (len == 0);
+        }
+    }
+    for (int64_t k = t0; k < nnz; k += stride) {
+        const int64_t c = idx(col[k]);
+        if (c < 0) ++v[1];
+        else v[2] = (unsigned long long)c > v[2] ? (unsigned long long)c : v[2];
+    }
+    __shared__ unsigned long long red[6][kCheckThreads / 32];
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+        for (int o = 16; o > 0; o >>= 1) v[f] = check_fold(f, v[f], __shfl_xor_sync(0xffffffffu, v[f], o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) red[f][warp] = v[f];
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int f = threadIdx.x;
+        unsigned long long a = red[f][0];
+        for (int w = 1; w < kCheckThreads / 32; ++w) a = check_fold(f, a, red[f][w]);
+        part[(int64_t)blockIdx.x * 6 + f] = a;
+    }
+}
+
+template <class P>
+__global__ void __launch_bounds__(kCheckThreads) k_csr_check_final(const P* __restrict__ ptr, int64_t n_rows,
+                                                                    const unsigned long long* __restrict__ part,
+                                                                    int n_parts, int64_t* out) {
+    __shared__ unsigned long long red[6][kCheckThreads / 32];
+    unsigned long long v[6] = {0, 0, 0, 0, 0, 0};
+    for (int b = threadIdx.x; b < n_parts; b += blockDim.x)
+#pragma unroll
+        for (int f = 0; f < 6; ++f) v[f] = check_fold(f, v[f], part[(int64_t)b * 6 + f]);
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+        for (int o = 16; o > 0; o >>= 1) v[f] = check_fold(f, v[f], __shfl_xor_sync(0xffffffffu, v[f], o));
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+#pragma unroll
+        for (int f = 0; f < 6; ++f) red[f][warp] = v[f];
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        const int f = threadIdx.x;
+        unsigned long long a = red[f][0];
+        for (int w = 1; w < kCheckThreads / 32; ++w) a = check_fold(f, a, red[f][w]);
+        out[2 + f] = (int64_t)a;
+    } else if (threadIdx.x == 32) {
+        out[0] = idx(ptr[0]);
+        out[1] = idx(ptr[n_rows]);
+    }
+}
+
+static int64_t check_blocks(int64_t n_rows, int64_t nnz) {
+    const int64_t work = n_rows > nnz ? n_rows : nnz;
+    const int64_t b = ceil_div(work, (int64_t)kCheckThreads * 8);
+    return b < 1 ? 1 : (b > kCheckMaxBlocks ? kCheckMaxBlocks : b);
+}
+
 }  // namespace fsb
 
 using namespace fsb;
@@ -119,6 +209,40 @@ extern "C" int fsb_merge_runs(const void* row_ptr, int ptr_dtype, int64_t n_rows
         k_merge_runs<P><<<(unsigned)ceil_div(n_units, 256), 256, 0, st>>>(static_cast<const P*>(row_ptr), n_rows,
                                                                          unit_coords, n_units, unit_runs);
         return fsb_host::check_launch("k_merge_runs");
+    });
+}
+
+extern "C" int64_t fsb_csr_check_workspace_bytes(int64_t n_rows, int64_t nnz) {
+    if (n_rows < 0 || nnz < 0) return 0;
+    return check_blocks(n_rows, nnz) * 6 * (int64_t)sizeof(unsigned long long);
+}
+
+extern "C" int fsb_csr_check(const void* row_ptr, int ptr_dtype, int64_t n_rows, const void* col_idx, int index_dtype,
+                             int64_t nnz, int64_t* out, void* workspace, int64_t workspace_bytes, void* stream) {
+    if (!row_ptr || !out || n_rows < 0 || nnz < 0 || (nnz > 0 && !col_idx)) {
+        fsb_host::set_error("fsb_csr_check: bad arguments");
+        return FSB_ERR_INVALID;
+    }
+    const int64_t blocks = check_blocks(n_rows, nnz);
+    if (!workspace || workspace_bytes < blocks * 6 * (int64_t)sizeof(unsigned long long)) {
+        fsb_host::set_error("fsb_csr_check: workspace %lld bytes < %lld", (long long)workspace_bytes,
+                            (long long)(blocks * 6 * (int64_t)sizeof(unsigned long long)));
+        return FSB_ERR_WORKSPACE;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned long long* part = static_cast<unsigned long long*>(workspace);
+    return dispatch_idx(ptr_dtype, [&](auto tp) -> int {
+        using P = typename decltype(tp)::type;
+        int rc = dispatch_idx(nnz > 0 ? index_dtype : FSB_I32, [&](auto ti) -> int {
+            using I = typename decltype(ti)::type;
+            k_csr_check_part<P, I><<<(unsigned)blocks, kCheckThreads, 0, st>>>(
+                static_cast<const P*>(row_ptr), n_rows, static_cast<const I*>(col_idx), nnz, part);
+            return fsb_host::check_launch("k_csr_check_part");
+        });
+        if (rc) return rc;
+        k_csr_check_final<P><<<1, kCheckThreads, 0, st>>>(static_cast<const P*>(row_ptr), n_rows, part,
+                                                          (int)blocks, out);
+        return fsb_host::check_launch("k_csr_check_final");
     });
 }
 

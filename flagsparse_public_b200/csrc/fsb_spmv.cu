@@ -16,6 +16,8 @@
 // FlagSparse computes the same products in _spmv_csr_real_kernel
 // (spmv_csr.py:158-184), _spmv_csr_complex_kernel (:187-219), the CSR-vector
 // bucket kernels (:225-343) and the COO row-run kernels (spmv_coo.py:131-226).
+#include <cstring>
+#include <cmath>
 #include <mutex>
 
 #include "fsb_partition.cuh"
@@ -26,6 +28,10 @@ constexpr int kRowsThreads = 256;
 constexpr int kMergeThreads = 128;
 constexpr int kMergeMaxItemsPerThread = 8;
 constexpr int kMergeMaxTile = kMergeThreads * kMergeMaxItemsPerThread;
+// FSB_PLAN_OVERLAP_LAUNCH applies to grids of at most one wave at four
+// resident CTAs per SM (a waiting successor then takes no slot a later wave
+// of this kernel would need)
+constexpr int64_t kOverlapMaxBlocks = 148 * 4;
 
 // Partial sum of row nonzeros [s, e) handled by `lane` of a T-lane group.
 // VEC-wide aligned body, scalar head and tail.
@@ -71,7 +77,14 @@ template <class V, class A, class O, class I, class P>
 __global__ void __launch_bounds__(kRowsThreads)
 k_spmv_rows(const V* __restrict__ val, const I* __restrict__ col, const P* __restrict__ ptr,
             const I* __restrict__ row_map, const V* __restrict__ x, O* __restrict__ y,
-            int64_t n_rows, int64_t row_cap, int64_t comp_threshold, int lanes_log2, int vec_ok) {
+            int64_t n_rows, int64_t row_cap, int64_t comp_threshold, int lanes_log2, int vec_ok, int overlap) {
+    if (overlap) {
+        // programmatic dependent launch: let the next launch on the stream
+        // start its CTAs now, and wait here until the previous kernel has
+        // completed and its writes are visible -- nothing is read before
+        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+        asm volatile("griddepcontrol.wait;" ::: "memory");
+    }
     const int T = 1 << lanes_log2;
     const int wl = threadIdx.x & 31;
     const int lane = wl & (T - 1);
@@ -286,8 +299,28 @@ extern "C" int fsb_spmv_csr(const fsb_csr* A, const void* x, void* y, int out_dt
                     if (plan->grid_blocks > 0 && grid > plan->grid_blocks) grid = plan->grid_blocks;
                     if (grid > 0x7fffffffLL) grid = 0x7fffffffLL;
                     const int64_t thr = plan->comp_threshold > 0 ? plan->comp_threshold : 0;
-                    k_spmv_rows<V, Ac, O, I, P><<<(unsigned)grid, kRowsThreads, 0, st>>>(
-                        val, col, ptr, rmap, xv, yv, A->n_rows, plan->row_cap, thr, lg, vec_ok);
+                    const int overlap = (plan->flags & FSB_PLAN_OVERLAP_LAUNCH) && grid <= kOverlapMaxBlocks;
+                    if (!overlap) {
+                        k_spmv_rows<V, Ac, O, I, P><<<(unsigned)grid, kRowsThreads, 0, st>>>(
+                            val, col, ptr, rmap, xv, yv, A->n_rows, plan->row_cap, thr, lg, vec_ok, 0);
+                        return fsb_host::check_launch("k_spmv_rows");
+                    }
+                    cudaLaunchConfig_t cfg = {};
+                    cfg.gridDim = dim3((unsigned)grid);
+                    cfg.blockDim = dim3(kRowsThreads);
+                    cfg.stream = st;
+                    cudaLaunchAttribute attr[1];
+                    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+                    attr[0].val.programmaticStreamSerializationAllowed = 1;
+                    cfg.attrs = attr;
+                    cfg.numAttrs = 1;
+                    const int64_t nr = A->n_rows, rc_cap = plan->row_cap;
+                    const cudaError_t e = cudaLaunchKernelEx(&cfg, k_spmv_rows<V, Ac, O, I, P>, val, col, ptr, rmap,
+                                                             xv, yv, nr, rc_cap, thr, lg, vec_ok, 1);
+                    if (e != cudaSuccess) {
+                        fsb_host::set_error("k_spmv_rows (overlapped launch): %s", cudaGetErrorString(e));
+                        return FSB_ERR_LAUNCH;
+                    }
                     return fsb_host::check_launch("k_spmv_rows");
                 }
                 if (plan->algo != FSB_ALGO_MERGE) {
@@ -332,6 +365,104 @@ extern "C" int fsb_spmv_csr(const fsb_csr* A, const void* x, void* y, int out_dt
             });
         });
     });
+}
+
+// ------------------------------------------------------ one-shot SpMV ----
+// fsb_spmv_csr_checked: structural check, one device->host read of its
+// figures, the heuristic plan from them, the product -- one host call.
+
+namespace {
+int64_t check_bytes(const fsb_csr* A) { return align_up(fsb_csr_check_workspace_bytes(A->n_rows, A->nnz), 256); }
+
+// Row-group width / merge-path choice from the check's figures: merge path
+// for skewed rows that are short on average, else 2 * mean / (16-byte vector
+// elements) lanes rounded to a power of two in [2, 32] (ties to even).
+void checked_plan(const fsb_csr* A, const int64_t* fig, fsb_plan* plan) {
+    memset(plan, 0, sizeof(*plan));
+    const int esz = elem_size(A->value_dtype);
+    const int vec = esz >= 16 ? 1 : 16 / esz;
+    const double mean = A->n_rows ? (double)A->nnz / (double)A->n_rows : 0.0;
+    const bool skewed = (double)fig[5] > 8.0 * (mean > 1.0 ? mean : 1.0) + 256.0;
+    if (A->n_rows > 0 && skewed && mean < 32.0) {
+        plan->algo = FSB_ALGO_MERGE;
+        plan->items_per_unit = kMergeThreads * (esz <= 4 ? 8 : 4);
+        plan->n_units = ceil_div(A->n_rows + A->nnz, plan->items_per_unit);
+        return;
+    }
+    double v = A->n_rows ? 2.0 * mean / vec : 32.0;
+    if (v < 1.0) v = 1.0;
+    int lanes = 1 << (int)std::nearbyint(std::log2(v));
+    plan->algo = FSB_ALGO_ROWS;
+    plan->lanes = lanes < 2 ? 2 : (lanes > 32 ? 32 : lanes);
+    plan->flags = FSB_PLAN_OVERLAP_LAUNCH;
+}
+
+int64_t checked_merge_bytes(const fsb_csr* A, int acc_mode, int out_dtype) {
+    fsb_plan mp;
+    memset(&mp, 0, sizeof(mp));
+    mp.algo = FSB_ALGO_MERGE;
+    mp.items_per_unit = kMergeThreads * (elem_size(A->value_dtype) <= 4 ? 8 : 4);
+    mp.n_units = ceil_div(A->n_rows + A->nnz, mp.items_per_unit);
+    const int64_t coords = align_up((mp.n_units + 1) * 2 * (int64_t)sizeof(int64_t), 256);
+    return coords + fsb_workspace_bytes(0, A, 1, acc_mode, out_dtype, &mp);
+}
+}  // namespace
+
+extern "C" int64_t fsb_spmv_csr_checked_workspace_bytes(const fsb_csr* A, int acc_mode, int out_dtype) {
+    if (!A || A->n_rows < 0 || A->nnz < 0) return 0;
+    return check_bytes(A) + checked_merge_bytes(A, acc_mode, out_dtype);
+}
+
+extern "C" int fsb_spmv_csr_checked(const fsb_csr* A, const void* x, void* y, int out_dtype, int acc_mode,
+                                    void* workspace, int64_t workspace_bytes, int64_t* figures, fsb_plan* plan_out,
+                                    void* stream) {
+    if (!A || !figures || A->n_rows < 0 || A->nnz < 0) {
+        fsb_host::set_error("fsb_spmv_csr_checked: bad arguments");
+        return FSB_ERR_INVALID;
+    }
+    const int64_t need = fsb_spmv_csr_checked_workspace_bytes(A, acc_mode, out_dtype);
+    if (!workspace || workspace_bytes < need) {
+        fsb_host::set_error("fsb_spmv_csr_checked: workspace %lld bytes < %lld", (long long)workspace_bytes,
+                            (long long)need);
+        return FSB_ERR_WORKSPACE;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // the check's kernels write the figures straight into a pinned buffer of
+    // this host thread: no copy-engine work to queue behind uploads
+    static thread_local int64_t* staged = nullptr;
+    if (!staged && cudaHostAlloc(reinterpret_cast<void**>(&staged), 8 * sizeof(int64_t),
+                                 cudaHostAllocMapped | cudaHostAllocPortable) != cudaSuccess) {
+        staged = nullptr;
+        return fsb_host::check_launch("fsb_spmv_csr_checked: pinned figure buffer");
+    }
+    const int64_t cb = check_bytes(A);
+    int rc = fsb_csr_check(A->row_ptr, A->ptr_dtype, A->n_rows, A->col_idx, A->index_dtype, A->nnz, staged,
+                           workspace, cb, stream);
+    if (rc) return rc;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return fsb_host::check_launch("fsb_spmv_csr_checked: check");
+    memcpy(figures, staged, 8 * sizeof(int64_t));
+    if (figures[0] != 0 || figures[1] != A->nnz || figures[2] != 0 ||
+        (A->nnz > 0 && (figures[3] != 0 || figures[4] >= A->n_cols))) {
+        fsb_host::set_error("fsb_spmv_csr_checked: malformed CSR structure (figures returned)");
+        return FSB_ERR_INVALID;
+    }
+    fsb_plan plan;
+    checked_plan(A, figures, &plan);
+    if (plan_out) *plan_out = plan;
+    if (A->n_rows == 0) return FSB_OK;
+    char* rest = static_cast<char*>(workspace) + cb;
+    int64_t rest_bytes = workspace_bytes - cb;
+    if (plan.algo == FSB_ALGO_MERGE) {
+        int64_t* coords = reinterpret_cast<int64_t*>(rest);
+        const int64_t cb = align_up((plan.n_units + 1) * 2 * (int64_t)sizeof(int64_t), 256);
+        rc = fsb_merge_partition(A->row_ptr, A->ptr_dtype, A->n_rows, A->nnz, plan.items_per_unit, 0, coords,
+                                 plan.n_units, stream);
+        if (rc) return rc;
+        plan.unit_coords = coords;
+        rest += cb;
+        rest_bytes -= cb;
+    }
+    return fsb_spmv_csr(A, x, y, out_dtype, acc_mode, &plan, rest, rest_bytes, stream);
 }
 
 // --------------------------------------------------- allocation-free SpMV ----

@@ -117,12 +117,3 @@ def _benchmark_cuda_op(op, warmup, iters):
     return output, elapsed_ms
 
 
-def _device_checks(checks):
-    """Evaluate several scalar device checks with one device->host read.
-
-    ``checks`` is a list of 0-d tensors (bool or integer); returns Python values.
-    """
-    if not checks:
-        return []
-    vals = torch.stack([c.to(torch.int64) for c in checks]).tolist()
-    return vals

@@ -62,8 +62,10 @@ def prepare_csr_mixed(data, indices, indptr, shape, compensate_above=COMPENSATE_
         raise ValueError("compensate_above must be non-negative")
     if layout not in LAYOUTS:
         raise ValueError(f"layout must be one of {LAYOUTS}")
-    data, kidx, kptr, n_rows, n_cols, _lens, max_row = _prepare_spmv_csr_matrix(data, indices, indptr, shape)
+    data, kidx, kptr, n_rows, n_cols, _lens, max_row, stats = _prepare_spmv_csr_matrix(data, indices, indptr, shape,
+                                                                                        return_stats=True)
     p = PreparedCsrMixed(data, kidx, kptr, shape, n_rows, n_cols, max_row, compensate_above, layout)
+    p._stats = stats
     if layout != "csr":
         _structured_form(p)
     return p

@@ -16,7 +16,6 @@ copies of A and B; the opt path accumulates in the value precision (``:631``).
 import math
 
 from ._common import *
-from ._common import _device_checks
 from .. import _native as _nat
 from .. import _plan
 
@@ -100,8 +99,8 @@ def _spmm_validation_metrics(candidate, reference):
 
 
 def _prepare_spmm_csr_matrix(data, indices, indptr, shape, return_stats=False):
-    """Validation of FlagSparse ``spmm_csr.py:197-255`` with one device->host
-    read for all structural checks.  Returns int32 column indices (int64 ones
+    """Validation of FlagSparse ``spmm_csr.py:197-255`` with one kernel and
+    one device->host read for all structural checks.  Returns int32 column indices (int64 ones
     converted, as the reference does) and int64 indptr; with ``return_stats``
     also the row-length statistics of the plan heuristics, from the same read."""
     if len(shape) != 2:
@@ -127,38 +126,27 @@ def _prepare_spmm_csr_matrix(data, indices, indptr, shape, return_stats=False):
         raise TypeError("indptr dtype must be torch.int32 or torch.int64")
 
     nnz = data.numel()
-    zero = torch.zeros((), dtype=torch.int64, device=data.device)
-    row_lengths = (indptr[1:] - indptr[:-1]).to(torch.int64) if n_rows > 0 else zero.new_empty((0,))
-    checks = [indptr[0], indptr[-1], (row_lengths < 0).any() if n_rows > 0 else zero]
-    if nnz > 0:
-        checks += [indices.min(), indices.max()]
-    checks.append(row_lengths.max() if n_rows > 0 else zero)
-    if return_stats:
-        checks += [(row_lengths * row_lengths).sum() if n_rows > 0 else zero,
-                   (row_lengths == 0).sum() if n_rows > 0 else zero]
-    vals = _device_checks(checks)
-    if indptr.numel() > 0 and int(vals[0]) != 0:
-        raise ValueError("indptr[0] must be 0")
-    if indptr.numel() > 0 and int(vals[1]) != nnz:
-        raise ValueError(f"indptr[-1] must equal nnz={nnz}, got {int(vals[1])}")
-    if indptr.numel() > 1 and vals[2]:
-        raise ValueError("indptr must be nondecreasing")
-    if nnz > 0:
-        min_col, max_col = int(vals[3]), int(vals[4])
-        if min_col < 0 or max_col >= n_cols:
-            raise IndexError("indices out of range for n_cols")
-        if max_col > _INDEX_LIMIT_INT32:
-            raise ValueError("column indices exceed the int32 range supported by the Triton kernel")
-
     data = data.contiguous()
     indices = indices.contiguous()
     indptr = indptr.contiguous()
+    # every structural check in one kernel and one device->host read (fsb_csr_check)
+    c = _nat.csr_check(indptr, indices, n_rows)
+    if c[0] != 0:
+        raise ValueError("indptr[0] must be 0")
+    if c[1] != nnz:
+        raise ValueError(f"indptr[-1] must equal nnz={nnz}, got {c[1]}")
+    if c[2]:
+        raise ValueError("indptr must be nondecreasing")
+    if nnz > 0:
+        if c[3] or c[4] >= n_cols:
+            raise IndexError("indices out of range for n_cols")
+        if c[4] > _INDEX_LIMIT_INT32:
+            raise ValueError("column indices exceed the int32 range supported by the Triton kernel")
+    row_lengths = (indptr[1:] - indptr[:-1]).to(torch.int64)
     kernel_indices = indices.to(torch.int32) if indices.dtype == torch.int64 else indices
     kernel_indptr = indptr.to(torch.int64)
-    if return_stats:
-        sum_sq, empty = vals[-2], vals[-1]
-        vals = vals[:-2]
-    max_row_nnz = int(vals[-1]) if n_rows > 0 else 0
+    max_row_nnz = c[5]
+    sum_sq, empty = c[6], c[7]
     if not return_stats:
         return data, kernel_indices, kernel_indptr, n_rows, n_cols, row_lengths, max_row_nnz
     if n_rows == 0:

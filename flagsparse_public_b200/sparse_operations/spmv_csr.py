@@ -16,8 +16,10 @@ copies of the matrix and of x; the ``use_opt`` path accumulates float32 in
 float32 (``spmv_csr.py:246``).
 """
 
+import ctypes
+import math
+
 from ._common import *
-from ._common import _device_checks
 from .. import _native as _nat
 from .. import _plan
 
@@ -161,15 +163,16 @@ def _spmv_plan(prepared, kind, row_cap=0):
     return plan
 
 
-def _build_spmv_opt_buckets(row_lengths, max_row_nnz, row_index_dtype, max_segments=None, fp64=False):
-    """Plan description of the opt path (FlagSparse kept per-tier row lists here).
+def _build_spmv_opt_buckets(n_rows, max_row_nnz, row_index_dtype, max_segments=None, fp64=False):
+    """Plan description of the opt path (FlagSparse kept per-tier row lists
+    here, built from the row lengths; this one takes the row count).
 
     The kernels of this implementation need no row lists: one launch covers
     all rows (row groups sized from the mean row length, or merge-path tiles
     for skewed rows).  The returned list describes that launch.
     """
     del row_index_dtype, max_segments, fp64
-    n_rows = int(row_lengths.numel())
+    n_rows = int(n_rows)
     if n_rows == 0:
         return []
     return [{"kind": "single_launch", "rows": n_rows, "max_row_nnz": int(max_row_nnz)}]
@@ -218,7 +221,7 @@ def _transpose_csr_for_spmv(data, indices, indptr, shape):
     )
 
 
-def _prepare_spmv_csr_matrix(data, indices, indptr, shape, index_fallback_policy="auto"):
+def _prepare_spmv_csr_matrix(data, indices, indptr, shape, index_fallback_policy="auto", return_stats=False):
     _normalize_spmv_index_fallback_policy(index_fallback_policy)
     if not all(torch.is_tensor(t) for t in (data, indices, indptr)):
         raise TypeError("data, indices, indptr must all be torch.Tensor")
@@ -245,24 +248,28 @@ def _prepare_spmv_csr_matrix(data, indices, indptr, shape, index_fallback_policy
     indptr = indptr.contiguous()
     nnz = data.numel()
 
-    # All structural checks in one device->host read, raised in FlagSparse's order.
-    row_lengths = indptr[1:] - indptr[:-1]
-    checks = [indptr[0], indptr[-1]]
-    checks.append((row_lengths < 0).any() if n_rows > 0 else torch.zeros((), device=data.device))
-    if nnz > 0:
-        checks += [indices.min(), indices.max()]
-    checks.append(row_lengths.max() if n_rows > 0 else torch.zeros((), device=data.device))
-    vals = _device_checks(checks)
-    if int(vals[0]) != 0:
+    # All structural checks in one kernel and one device->host read
+    # (fsb_csr_check), raised in FlagSparse's order.
+    c = _nat.csr_check(indptr, indices, n_rows)
+    if c[0] != 0:
         raise ValueError("indptr must start at zero")
-    if int(vals[1]) != nnz:
+    if c[1] != nnz:
         raise ValueError("indptr[-1] must equal nnz")
-    if indptr.numel() > 1 and vals[2]:
+    if c[2]:
         raise ValueError("indptr must be non-decreasing")
-    if nnz > 0 and (vals[3] < 0 or vals[4] >= n_cols):
+    if nnz > 0 and (c[3] or c[4] >= n_cols):
         raise IndexError("indices out of range for n_cols")
-    max_row_nnz = int(vals[-1]) if n_rows > 0 else 0
-    return data, indices, indptr, n_rows, n_cols, row_lengths, max_row_nnz
+    max_row_nnz = c[5]
+    # row lengths are not materialised: the kernels read the row offsets
+    if not return_stats:
+        return data, indices, indptr, n_rows, n_cols, None, max_row_nnz
+    if n_rows == 0:
+        stats = _plan.MatrixStats(0, n_cols, 0, 0, 0.0, 0.0, 0)
+    else:
+        mean = nnz / n_rows
+        std = math.sqrt(max(c[6] / n_rows - mean * mean, 0.0))
+        stats = _plan.MatrixStats(n_rows, n_cols, nnz, max_row_nnz, mean, std, c[7])
+    return data, indices, indptr, n_rows, n_cols, None, max_row_nnz, stats
 
 
 def _validate_spmv_x(x, prepared):
@@ -304,8 +311,9 @@ def prepare_spmv_csr(
         if op_code == SPMV_OP_CONJ_TRANS and _is_complex_dtype(data.dtype):
             data = data.conj().resolve_conj()
         data, indices, indptr, shape = _transpose_csr_for_spmv(data, indices, indptr, shape)
-    (data, kernel_indices, kernel_indptr, n_rows, n_cols, row_lengths, max_row_nnz) = _prepare_spmv_csr_matrix(
-        data, indices, indptr, shape, index_fallback_policy=index_fallback_policy
+    (data, kernel_indices, kernel_indptr, n_rows, n_cols, _row_lengths, max_row_nnz,
+     stats) = _prepare_spmv_csr_matrix(
+        data, indices, indptr, shape, index_fallback_policy=index_fallback_policy, return_stats=True
     )
     block_nnz_use = block_nnz
     if max_segments is None:
@@ -317,7 +325,7 @@ def prepare_spmv_csr(
         max_segments_use = max_segments
     row_index_dtype = torch.int32 if n_rows <= _INDEX_LIMIT_INT32 else torch.int64
     opt_buckets = _build_spmv_opt_buckets(
-        row_lengths, max_row_nnz=max_row_nnz, row_index_dtype=row_index_dtype, max_segments=max_segments,
+        n_rows, max_row_nnz=max_row_nnz, row_index_dtype=row_index_dtype, max_segments=max_segments,
         fp64=data.dtype == torch.float64,
     )
     prepared = PreparedCsrSpmv(
@@ -336,6 +344,7 @@ def prepare_spmv_csr(
         index_fallback_policy=index_fallback_policy,
     )
     prepared._explicit_max_segments = max_segments
+    prepared._stats = stats
     return prepared
 
 
@@ -444,11 +453,10 @@ def _spmv_prepared_with_int32_indices(prepared, reason):
         raise RuntimeError(f"native int64 CSR SpMV failed and int32 fallback is unsafe: {blocker}")
     kernel_indices = prepared.kernel_indices.to(torch.int32)
     kernel_indptr = prepared.kernel_indptr.to(torch.int32)
-    row_lengths = kernel_indptr[1:] - kernel_indptr[:-1]
-    max_row_nnz = int(row_lengths.max().item()) if prepared.n_rows > 0 else 0
+    max_row_nnz = prepared.max_row_nnz
     row_index_dtype = torch.int32 if prepared.n_rows <= _INDEX_LIMIT_INT32 else torch.int64
     opt_buckets = _build_spmv_opt_buckets(
-        row_lengths, max_row_nnz=max_row_nnz, row_index_dtype=row_index_dtype,
+        prepared.n_rows, max_row_nnz=max_row_nnz, row_index_dtype=row_index_dtype,
         max_segments=prepared.max_segments, fp64=prepared.data.dtype == torch.float64,
     )
     fallback = PreparedCsrSpmv(
@@ -472,20 +480,39 @@ def _spmv_prepared_with_int32_indices(prepared, reason):
     return fallback
 
 
-def _run_spmv_prepared(prepared, x, use_opt=False):
-    if use_opt and prepared.supports_opt:
-        return _triton_spmv_csr_impl_opt_prepared(prepared, x)
-    return _triton_spmv_csr_impl_prepared(prepared, x)
+def _run_spmv_prepared(prepared, x, use_opt=False, out=None):
+    impl = _triton_spmv_csr_impl_opt_prepared if use_opt and prepared.supports_opt else _triton_spmv_csr_impl_prepared
+    return impl(prepared, x) if out is None else impl(prepared, x, out=out)
 
 
-def _run_spmv_prepared_with_fallback(prepared, x, use_opt=False):
+def _run_spmv_prepared_with_fallback(prepared, x, use_opt=False, out=None):
+    # ``out`` is passed only when given: the hook keeps FlagSparse's signature
+    kw = {} if out is None else {"out": out}
     try:
-        return _run_spmv_prepared(prepared, x, use_opt=use_opt)
+        return _run_spmv_prepared(prepared, x, use_opt=use_opt, **kw)
     except Exception as exc:
         if prepared.index_fallback_policy != "auto" or not _spmv_uses_int64_indices(prepared):
             raise
         fallback_prepared = _spmv_prepared_with_int32_indices(prepared, exc)
-        return _run_spmv_prepared(fallback_prepared, x, use_opt=use_opt)
+        return _run_spmv_prepared(fallback_prepared, x, use_opt=use_opt, **kw)
+
+
+def _direct_out(out, prepared, x):
+    """``out`` itself as the kernel's output when it has exactly the result's
+    layout and shares no memory with the operands; otherwise None and the
+    result is computed separately and copied into ``out`` (FlagSparse's
+    behaviour, ``spmv_csr.py:861-869``), which keeps y = A y correct."""
+    if (out is None or not torch.is_tensor(out) or not out.is_cuda or out.device != prepared.data.device
+            or out.dtype != prepared.data.dtype or tuple(out.shape) != (prepared.n_rows,)
+            or not out.is_contiguous()):
+        return None
+    a0 = out.data_ptr()
+    a1 = a0 + out.numel() * out.element_size()
+    for t in (x, prepared.data, prepared.kernel_indices, prepared.kernel_indptr):
+        b0 = t.data_ptr()
+        if t.numel() and a0 < b0 + t.numel() * t.element_size() and b0 < a1:
+            return None
+    return out
 
 
 def flagsparse_spmv_csr(
@@ -518,6 +545,10 @@ def flagsparse_spmv_csr(
     if prepared is None:
         if any(arg is None for arg in (data, indices, indptr, shape)):
             raise ValueError("data, indices, indptr, and shape are required when prepared is not provided")
+        if op_code == SPMV_OP_NON and max_segments is None and not return_time:
+            y = _spmv_csr_checked(data, indices, indptr, x, shape, use_opt, index_fallback_policy)
+            if y is not None:
+                return _spmv_write_out(y, out)
         prepared = prepare_spmv_csr(
             data, indices, indptr, shape, block_nnz=block_nnz, max_segments=max_segments, op=op_code,
             index_fallback_policy=index_fallback_policy,
@@ -536,12 +567,19 @@ def flagsparse_spmv_csr(
     if return_time:
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-    y = _run_spmv_prepared_with_fallback(prepared, x, use_opt=use_opt)
+    y = _run_spmv_prepared_with_fallback(prepared, x, use_opt=use_opt, out=_direct_out(out, prepared, x))
     elapsed_ms = None
     if return_time:
         torch.cuda.synchronize()
         elapsed_ms = (time.perf_counter() - t0) * 1000.0
-    if out is not None:
+    y = _spmv_write_out(y, out)
+    if return_time:
+        return y, elapsed_ms
+    return y
+
+
+def _spmv_write_out(y, out):
+    if out is not None and y is not out:
         if not out.is_cuda:
             raise ValueError("out must be a CUDA tensor")
         if out.device != y.device:
@@ -550,8 +588,55 @@ def flagsparse_spmv_csr(
             raise ValueError("out shape/dtype must match result")
         out.copy_(y)
         y = out
-    if return_time:
-        return y, elapsed_ms
+    return y
+
+
+def _spmv_csr_checked(data, indices, indptr, x, shape, use_opt, index_fallback_policy):
+    """One-shot y = A x in one native call (fsb_spmv_csr_checked): the
+    structural check, its single device->host read, the heuristic plan and
+    the product.  Returns None when the call needs the general route: int64
+    column indices (FlagSparse's int32 index fallback applies there), an x
+    the prepared route would reject, or anything the argument checks below do
+    not cover -- that route then raises FlagSparse's errors in its order."""
+    _normalize_spmv_index_fallback_policy(index_fallback_policy)
+    if not all(torch.is_tensor(t) for t in (data, indices, indptr, x)) or len(shape) != 2:
+        return None
+    n_rows, n_cols = int(shape[0]), int(shape[1])
+    dtype = data.dtype
+    if (data.ndim != 1 or indices.ndim != 1 or indptr.ndim != 1 or x.ndim != 1 or indptr.numel() != n_rows + 1
+            or data.numel() != indices.numel() or indices.dtype != torch.int32
+            or indptr.dtype not in SUPPORTED_INDEX_DTYPES or dtype not in SUPPORTED_SPMV_VALUE_DTYPES
+            or x.dtype != dtype or x.numel() != n_cols or not data.is_cuda
+            or not all(t.device == data.device for t in (indices, indptr, x))):
+        return None
+    data, indices, indptr, x = data.contiguous(), indices.contiguous(), indptr.contiguous(), x.contiguous()
+    if use_opt and dtype in (torch.float32, torch.float64):
+        acc = _nat.ACC_NATIVE
+    else:
+        acc = _nat.ACC_WIDE if dtype == torch.float32 else _nat.ACC_NATIVE
+    y = torch.empty(n_rows, dtype=dtype, device=data.device)
+    cm = _nat.make_csr(data, indices, indptr, n_rows, n_cols)
+    out_code = _nat.dtype_code(dtype)
+    lib = _nat.library()
+    nbytes = int(lib.fsb_spmv_csr_checked_workspace_bytes(cm, acc, out_code))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=data.device)
+    fig = (ctypes.c_int64 * 8)()
+    fig[7] = -1  # empty-row count: >= 0 once the figures were read
+    plan = _nat.FsbPlan()
+    rc = lib.fsb_spmv_csr_checked(cm, _nat.ptr(x), _nat.ptr(y), out_code, acc, _nat.ptr(ws), nbytes, fig, plan,
+                                  _nat.stream_handle(data.device))
+    if rc == _nat.FSB_ERR_INVALID and fig[7] >= 0:
+        # FlagSparse's messages, in its order (spmv_csr.py:524-537)
+        if fig[0] != 0:
+            raise ValueError("indptr must start at zero")
+        if fig[1] != data.numel():
+            raise ValueError("indptr[-1] must equal nnz")
+        if fig[2]:
+            raise ValueError("indptr must be non-decreasing")
+        raise IndexError("indices out of range for n_cols")
+    if rc != _nat.FSB_OK:
+        return None  # the general route retries (index fallback) or raises
+    _plan.LAUNCHES["count"] += 1 + (0 if n_rows == 0 else (1 if plan.algo == _nat.ALGO_ROWS else 3))
     return y
 
 

@@ -80,6 +80,16 @@ extern "C" {
                                   aligned B and C rows, else
                                   FSB_ERR_UNSUPPORTED                          */
 
+#define FSB_PLAN_OVERLAP_LAUNCH 2  /* ROWS SpMV of at most 592 CTAs: launched
+                                  with programmatic dependent launch, so its
+                                  CTAs may start while the previous kernel on
+                                  the stream drains; each waits for that
+                                  kernel's completion (griddepcontrol.wait)
+                                  before reading anything, and lets the next
+                                  such launch start early.  Hides the launch
+                                  gap of back-to-back SpMVs (solver loops,
+                                  CUDA graphs); results are unchanged       */
+
 /* A CSR matrix (or a sorted COO matrix seen as row runs).
  * row_ptr has n_rows + 1 entries.  If row_map is non-null, row r of this
  * structure is written to output row row_map[row_ptr[r]] (COO row runs:
@@ -164,6 +174,25 @@ int fsb_merge_partition(const void* row_ptr, int ptr_dtype, int64_t n_rows,
                         int64_t snap_threshold, int64_t* unit_coords,
                         int64_t n_units, void* stream);
 
+/* Structural check of a CSR matrix in two kernels (per-CTA figures into
+ * workspace, then one CTA folding them into out[]) in place of FlagSparse's
+ * separate device reductions and host reads (spmv_csr.py:524-541,
+ * spmm_csr.py:197-255).  No memset and no copy: out[] may be device memory
+ * or pinned host memory (read it after synchronising the stream), so the
+ * check never queues behind host<->device copies.  out: eight int64:
+ *   out[0] = row_ptr[0]             out[1] = row_ptr[n_rows]
+ *   out[2] = rows of negative length
+ *   out[3] = column indices below zero
+ *   out[4] = largest non-negative column index (0 when there is none)
+ *   out[5] = longest row            out[6] = sum of squared row lengths
+ *   out[7] = empty rows   (out[5..7] over the rows of non-negative length)
+ * workspace_bytes >= fsb_csr_check_workspace_bytes(n_rows, nnz).         */
+int64_t fsb_csr_check_workspace_bytes(int64_t n_rows, int64_t nnz);
+int fsb_csr_check(const void* row_ptr, int ptr_dtype, int64_t n_rows,
+                  const void* col_idx, int index_dtype, int64_t nnz,
+                  int64_t* out, void* workspace, int64_t workspace_bytes,
+                  void* stream);
+
 /* Split-row runs of a merge-path partition (unit_coords from
  * fsb_merge_partition for the same row_ptr): for every unit u whose end falls
  * inside a row r (after at least one of r's nonzeros), unit_runs[2*u] is the
@@ -174,6 +203,27 @@ int fsb_merge_partition(const void* row_ptr, int ptr_dtype, int64_t n_rows,
 int fsb_merge_runs(const void* row_ptr, int ptr_dtype, int64_t n_rows,
                    const int64_t* unit_coords, int64_t n_units,
                    int64_t* unit_runs, void* stream);
+
+/* One-shot SpMV with the structural check, for a matrix seen once (the
+ * reference's flagsparse_spmv_csr without `prepared`: prepare_spmv_csr's
+ * checks, spmv_csr.py:497-549, then the product, :796-872).  One host call:
+ * fsb_csr_check (partials in workspace) writing its eight figures to a
+ * pinned buffer of the calling thread, one stream synchronisation, the
+ * figures copied to figures[] (host memory); a
+ * malformed structure (row_ptr[0] != 0, row_ptr[n_rows] != nnz, a negative
+ * row length, a column outside [0, n_cols)) returns FSB_ERR_INVALID with
+ * nothing launched, so the caller raises its own error from the figures.
+ * Otherwise the plan follows from the figures (merge path when the longest
+ * row exceeds 8 x max(mean, 1) + 256 and the mean is below 32, else
+ * 2 x mean / (16-byte vector elements) lanes per row group, a power of two
+ * in [2, 32]), written to plan_out when non-null, and the product runs as
+ * fsb_spmv_csr.  workspace_bytes >= fsb_spmv_csr_checked_workspace_bytes.  */
+int64_t fsb_spmv_csr_checked_workspace_bytes(const fsb_csr* A, int acc_mode,
+                                             int out_dtype);
+int fsb_spmv_csr_checked(const fsb_csr* A, const void* x, void* y,
+                         int out_dtype, int acc_mode, void* workspace,
+                         int64_t workspace_bytes, int64_t* figures,
+                         fsb_plan* plan_out, void* stream);
 
 /* Allocation-free merge-path SpMV, y = A x, for callers that cannot allocate
  * device memory (a C program or plug-in handed device pointers by a host

@@ -181,6 +181,24 @@ def merge_runs(indptr, n_rows, coords):
     return runs
 
 
+def csr_check(indptr, indices):
+    """The structural figures FlagSparse's CSR validation reads one by one
+    (``spmv_csr.py:524-541``: indptr[0], indptr[-1], non-decreasing offsets,
+    index range; ``row_lengths.max()``) plus the row-length statistics of the
+    plan heuristics, as eight integers: row_ptr[0], row_ptr[-1], rows of
+    negative length, negative column indices, largest non-negative column
+    index, longest row, sum of squared row lengths, empty rows (the last three
+    over rows of non-negative length)."""
+    p = _host(indptr).to(torch.int64)
+    c = _host(indices).to(torch.int64)
+    lens = p[1:] - p[:-1]
+    ok = lens[lens >= 0]
+    nonneg = c[c >= 0]
+    return [int(p[0]), int(p[-1]), int((lens < 0).sum()), int((c < 0).sum()),
+            int(nonneg.max()) if nonneg.numel() else 0, int(ok.max()) if ok.numel() else 0,
+            int((ok * ok).sum()), int((ok == 0).sum())]
+
+
 def merge_partition(indptr, n_rows, nnz, items, snap=0):
     indptr = _host(indptr)
     total = n_rows + nnz

@@ -480,3 +480,139 @@ def test_sorted_coo_to_csr_is_graph_capturable():
     ref = torch.zeros(shape[0] + 1, dtype=torch.int64, device="cuda")
     ref[1:] = torch.cumsum(torch.bincount(row.long(), minlength=shape[0]), 0)
     assert torch.equal(captured[2], ref)
+
+
+def _malformed(kind):
+    d = torch.tensor([1.0, 2.0, 3.0], device=DEV)
+    i = torch.tensor([0, 1, 2], dtype=torch.int32, device=DEV)
+    p = torch.tensor([0, 2, 3], device=DEV)
+    if kind == "start":
+        p = torch.tensor([1, 2, 3], device=DEV)
+    elif kind == "end":
+        p = torch.tensor([0, 2, 2], device=DEV)
+    elif kind == "decreasing":
+        d = torch.tensor([1.0, 2.0], device=DEV)
+        i = torch.tensor([0, 1], dtype=torch.int32, device=DEV)
+        p = torch.tensor([0, 3, 2], device=DEV)
+    elif kind == "negative_col":
+        i = torch.tensor([0, -1, 2], dtype=torch.int32, device=DEV)
+    elif kind == "col_too_large":
+        i = torch.tensor([0, 1, 3], dtype=torch.int32, device=DEV)
+    return d, i, p, (2, 3)
+
+
+# FlagSparse's messages (spmv_csr.py:524-537, spmm_csr.py:228-237), raised
+# from the one-read structural check
+SPMV_MALFORMED = [("start", ValueError, "start at zero"), ("end", ValueError, "must equal nnz"),
+                  ("decreasing", ValueError, "non-decreasing"), ("negative_col", IndexError, "out of range"),
+                  ("col_too_large", IndexError, "out of range")]
+SPMM_MALFORMED = [("start", ValueError, "must be 0"), ("end", ValueError, "must equal nnz"),
+                  ("decreasing", ValueError, "nondecreasing"), ("negative_col", IndexError, "out of range"),
+                  ("col_too_large", IndexError, "out of range")]
+
+
+@pytest.mark.parametrize("kind,exc,msg", SPMV_MALFORMED)
+def test_spmv_rejects_malformed_structure(kind, exc, msg):
+    d, i, p, shape = _malformed(kind)
+    with pytest.raises(exc, match=msg):
+        fs.flagsparse_spmv_csr(d, i, p, torch.ones(3, device=DEV), shape)
+
+
+@pytest.mark.parametrize("kind,exc,msg", SPMM_MALFORMED)
+def test_spmm_rejects_malformed_structure(kind, exc, msg):
+    d, i, p, shape = _malformed(kind)
+    with pytest.raises(exc, match=msg):
+        fs.flagsparse_spmm_csr(d, i, p, torch.ones(3, 4, device=DEV), shape)
+
+
+def test_prepared_stats_from_the_validation_read():
+    """The plan statistics a prepare takes from its single read equal a
+    separate computation over the row lengths."""
+    from flagsparse_public_b200 import _plan, synthetic
+
+    d, i, p, shape = synthetic.zipf_powerlaw(5000, 5000, alpha=1.8, mean=12.0, cap=3000, seed=3, device=DEV)
+    for prep in (fs.prepare_spmv_csr(d, i, p, shape), fs.prepare_spmm_csr_opt(d, i, p, shape)):
+        got, ref = prep._stats, _plan.matrix_stats(p, shape[0], shape[1])
+        assert (got.n_rows, got.nnz, got.max_row, got.empty_rows) == (ref.n_rows, ref.nnz, ref.max_row,
+                                                                      ref.empty_rows)
+        assert got.mean_row == pytest.approx(ref.mean_row, rel=1e-12)
+        assert got.std_row == pytest.approx(ref.std_row, rel=1e-9)
+
+
+ONESHOT_CASES = [("poisson", torch.float32, torch.int64, True), ("poisson", torch.float32, torch.int32, False),
+                 ("skewed", torch.float32, torch.int64, True), ("skewed", torch.float64, torch.int32, False),
+                 ("poisson", torch.bfloat16, torch.int64, False), ("skewed", torch.float16, torch.int64, True),
+                 ("poisson", torch.complex64, torch.int64, False), ("dense_rows", torch.float32, torch.int64, True),
+                 ("empty", torch.float32, torch.int64, True)]
+
+
+def _oneshot_matrix(kind, dtype, ptr_dtype):
+    from flagsparse_public_b200 import synthetic
+
+    if kind == "poisson":
+        d, i, p, shape = synthetic.poisson_uniform(3000, 2000, mean=16.0, seed=5, device=DEV)
+    elif kind == "skewed":  # short rows on average, a few very long: merge path
+        d, i, p, shape = synthetic.zipf_powerlaw(6000, 6000, alpha=1.8, mean=6.0, cap=4000, seed=6, device=DEV)
+    elif kind == "dense_rows":
+        d, i, p, shape = synthetic.poisson_uniform(500, 4000, mean=300.0, seed=7, device=DEV)
+    else:  # rows without nonzeros only
+        n = 40
+        d, i = torch.zeros(0, device=DEV), torch.zeros(0, dtype=torch.int32, device=DEV)
+        p, shape = torch.zeros(n + 1, dtype=torch.int64, device=DEV), (n, 30)
+    if dtype.is_complex:
+        d = torch.complex(d, -0.5 * d)
+    return d.to(dtype), i.to(torch.int32), p.to(ptr_dtype), shape
+
+
+@pytest.mark.parametrize("kind,dtype,ptr_dtype,use_opt", ONESHOT_CASES)
+def test_spmv_oneshot_native_route_equals_prepared(kind, dtype, ptr_dtype, use_opt):
+    """The one-shot call (fsb_spmv_csr_checked: check, one read, plan, product
+    in one native call) returns bit for bit what prepare + run returns, with
+    the plan the prepared route's heuristic picks."""
+    from flagsparse_public_b200 import _native as nat
+    from flagsparse_public_b200 import _plan
+
+    d, i, p, shape = _oneshot_matrix(kind, dtype, ptr_dtype)
+    x = _random_dense((shape[1],), dtype)
+    before = _plan.LAUNCHES["count"]
+    y1 = fs.flagsparse_spmv_csr(d, i, p, x, shape, use_opt=use_opt)
+    assert _plan.LAUNCHES["count"] > before
+    prep = fs.prepare_spmv_csr(d, i, p, shape)
+    y2 = fs.flagsparse_spmv_csr(x=x, prepared=prep, use_opt=use_opt)
+    assert y1.dtype == y2.dtype and torch.equal(y1, y2)
+    # the native plan equals the prepared heuristic's
+    cm = nat.make_csr(d, i, p, shape[0], shape[1])
+    acc = nat.ACC_NATIVE if (use_opt and dtype in (torch.float32, torch.float64)) else (
+        nat.ACC_WIDE if dtype == torch.float32 else nat.ACC_NATIVE)
+    nbytes = int(nat.library().fsb_spmv_csr_checked_workspace_bytes(cm, acc, nat.dtype_code(dtype)))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=DEV)
+    fig = (nat.ctypes.c_int64 * 8)()
+    plan = nat.FsbPlan()
+    y3 = torch.empty_like(y1)
+    rc = nat.library().fsb_spmv_csr_checked(cm, nat.ptr(x), nat.ptr(y3), nat.dtype_code(dtype), acc, nat.ptr(ws),
+                                            nbytes, fig, plan, nat.stream_handle(DEV))
+    nat.check(rc, "fsb_spmv_csr_checked")
+    assert list(fig) == orc_csr_check(p, i)
+    ref = _plan.default_spmv_plan(prep._stats, dtype)
+    assert plan.algo == ref.algo and plan.flags == ref.flags
+    if ref.algo == nat.ALGO_ROWS:
+        assert plan.lanes == ref.lanes
+    else:
+        assert plan.items_per_unit == ref.items_per_unit
+    assert torch.equal(y3, y1)
+
+
+def orc_csr_check(p, i):
+    from oracle import oracle as orc
+
+    return orc.csr_check(p.cpu(), i.cpu())
+
+
+@pytest.mark.parametrize("index_dtype", [torch.int32, torch.int64], ids=["i32", "i64"])
+@pytest.mark.parametrize("kind,exc,msg", SPMV_MALFORMED)
+def test_spmv_malformed_both_routes(kind, exc, msg, index_dtype):
+    """int32 indices take the one-call native route, int64 the prepared
+    route; both raise FlagSparse's error."""
+    d, i, p, shape = _malformed(kind)
+    with pytest.raises(exc, match=msg):
+        fs.flagsparse_spmv_csr(d, i.to(index_dtype), p, torch.ones(3, device=DEV), shape)

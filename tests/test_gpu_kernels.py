@@ -257,6 +257,32 @@ def test_merge_runs_kernel_matches_oracle():
         assert torch.equal(plan.runs.cpu()[: ref.numel()], ref), (pattern, items, snap)
 
 
+def test_csr_check_kernel_matches_oracle():
+    """fsb_csr_check's eight figures equal the oracle's, valid and malformed
+    structures alike (decreasing offsets, negative and out-of-range columns,
+    empty matrices), int32 and int64 offsets and indices."""
+    cases = []
+    for pattern in ("skewed", "empty_rows", "long_rows", "all_empty"):
+        _d, indices, indptr, _shape = csr_from_lengths(EDGE_LENGTHS[pattern], 20000, seed=31)
+        cases.append((indptr, indices))
+    _d, indices, indptr, _shape = csr_from_lengths(EDGE_LENGTHS["skewed"], 20000, seed=32)
+    bad_ptr = indptr.clone()
+    bad_ptr[3] = bad_ptr[5] + 2  # rows 2 and 3 change length, one negative
+    bad_col = indices.to(torch.int64)
+    bad_col[::97] = -3
+    bad_col[5] = 1 << 40
+    cases += [(bad_ptr, indices), (indptr, bad_col), (bad_ptr + 1, indices),
+              (torch.zeros(1, dtype=torch.int64), torch.zeros(0, dtype=torch.int64)),
+              (torch.tensor([0, 0, 0]), torch.zeros(0, dtype=torch.int32))]
+    for k, (p, c) in enumerate(cases):
+        for pt, it in ((torch.int64, torch.int64), (torch.int32, torch.int32), (torch.int64, torch.int32)):
+            if it == torch.int32 and c.numel() and int(c.to(torch.int64).abs().max()) >= 2**31:
+                continue
+            hp, hc = p.to(pt), c.to(it)
+            got = nat.csr_check(hp.to(DEV), hc.to(DEV), hp.numel() - 1)
+            assert got == orc.csr_check(hp, hc), (k, pt, it)
+
+
 def _spmm_two_kernel(d, n_rows, n_cols, B, C, acc, plan):
     """The same SEQ plan with split rows finished by the separate fix-up
     kernel (no unit runs in the C plan)."""
@@ -316,3 +342,47 @@ def test_seq_in_kernel_finish_compensated_rows():
         C = torch.empty_like(ref)
         _plan.run_spmm(*d, n_rows, n_cols, Bd, C, nat.ACC_COMP, plan)
         assert torch.equal(C, ref), (items, snap)
+
+
+@pytest.mark.parametrize("captured", [False, True], ids=["eager", "graph"])
+def test_overlapped_launch_chain_equals_plain(captured):
+    """Back-to-back row SpMVs launched with programmatic dependent launch
+    (FSB_PLAN_OVERLAP_LAUNCH), each reading the previous one's output
+    (x_{k+1} = A x_k), equal the same chain launched plainly, bit for bit:
+    every CTA waits for its predecessor before reading."""
+    from flagsparse_public_b200 import synthetic
+
+    d, i, p, shape = synthetic.poisson_uniform(8192, 8192, mean=16.0, seed=11, device=DEV)
+    d = d * 0.25
+    x0 = synthetic.dense_vector(shape[1], seed=12, device=DEV)
+    steps = 12
+
+    def chain(flags):
+        plan = _plan.KernelPlan(nat.ALGO_ROWS, lanes=8, flags=flags)
+        bufs = [x0.clone()] + [torch.empty_like(x0) for _ in range(steps)]
+
+        def run():
+            for k in range(steps):
+                _plan.run_spmv(d, i, p, shape[0], shape[1], bufs[k], bufs[k + 1], nat.ACC_NATIVE, plan)
+
+        if captured:
+            s = torch.cuda.Stream()
+            s.wait_stream(torch.cuda.current_stream())
+            with torch.cuda.stream(s):
+                run()
+            torch.cuda.current_stream().wait_stream(s)
+            g = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(g):
+                run()
+            for b in bufs[1:]:
+                b.fill_(float("nan"))
+            g.replay()
+        else:
+            run()
+        torch.cuda.synchronize()
+        return torch.stack(bufs[1:])
+
+    plain = chain(0)
+    overlapped = chain(nat.PLAN_OVERLAP_LAUNCH)
+    assert torch.isfinite(plain).all()
+    assert torch.equal(plain, overlapped)
