@@ -78,13 +78,10 @@ __global__ void __launch_bounds__(kRowsThreads)
 k_spmv_rows(const V* __restrict__ val, const I* __restrict__ col, const P* __restrict__ ptr,
             const I* __restrict__ row_map, const V* __restrict__ x, O* __restrict__ y,
             int64_t n_rows, int64_t row_cap, int64_t comp_threshold, int lanes_log2, int vec_ok, int overlap) {
-    if (overlap) {
-        // programmatic dependent launch: let the next launch on the stream
-        // start its CTAs now, and wait here until the previous kernel has
-        // completed and its writes are visible -- nothing is read before
-        asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
-        asm volatile("griddepcontrol.wait;" ::: "memory");
-    }
+    // programmatic dependent launch: wait until the previous kernel on the
+    // stream has completed and its writes are visible -- nothing is read
+    // before -- and let the next launch start once this CTA's rows are done
+    if (overlap) asm volatile("griddepcontrol.wait;" ::: "memory");
     const int T = 1 << lanes_log2;
     const int wl = threadIdx.x & 31;
     const int lane = wl & (T - 1);
@@ -111,6 +108,7 @@ k_spmv_rows(const V* __restrict__ val, const I* __restrict__ col, const P* __res
             y[out_row] = Out<O, A>::cvt(acc);
         }
     }
+    if (overlap) asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 // ---------------------------------------------------------- merge path ----
