@@ -54,6 +54,8 @@ def parse_args(argv=None):
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--profile", action="store_true",
                     help="only warm-up + timed device steps (for a profiler launch list)")
+    ap.add_argument("--form", default=None,
+                    help="with --profile: time this extra form of the workload (e.g. spmv_bf16) instead of its step")
     ap.add_argument("--only", action="store_true",
                     help="measure the chosen workload alone (no side configurations, no selector check)")
     ap.add_argument("--plan", default=None,
@@ -1355,10 +1357,16 @@ def run_ours(args):
         wl.force_plan(parse_plan(args.plan))
 
     if args.profile:
+        fn = wl.step
+        if args.form:
+            forms = wl.extra_forms() if hasattr(wl, "extra_forms") else {}
+            if args.form not in forms:
+                raise SystemExit(f"workload {args.workload} has no form {args.form!r}: {sorted(forms)}")
+            fn = forms[args.form][0]
         for _ in range(args.warmup):
-            wl.step()
+            fn()
         torch.cuda.synchronize()
-        times = time_device_steps(wl.step, args.steps, flush)
+        times = time_device_steps(fn, args.steps, flush)
         if rank == 0:
             print(json.dumps({"profile_run": True, "ms_per_step": sum(times) / len(times)}), flush=True)
         return 0
