@@ -29,6 +29,7 @@ ACC_NATIVE, ACC_WIDE, ACC_COMP = 0, 1, 2
 ALGO_ROWS, ALGO_MERGE, ALGO_FLAT, ALGO_GATHER, ALGO_SEQ = 0, 1, 2, 3, 4
 PLAN_TMA_GATHER = 1  # fsb_plan.flags: SEQ with B rows staged by TMA tile::gather4
 PLAN_OVERLAP_LAUNCH = 2  # fsb_plan.flags: ROWS SpMV with programmatic dependent launch
+DIAG_NATIVE, DIAG_WIDE, DIAG_KAHAN, DIAG_KAHAN_WIDE = 0, 1, 2, 3  # fsb_spmm_csr_diag accumulations
 BSR_STAGE_TMA, BSR_STAGE_THREADS = 0, 1
 
 _DTYPE_CODES = {
@@ -150,6 +151,11 @@ _SIGNATURES = {
         ctypes.c_int,
         [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
          ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(FsbPlan), ctypes.c_void_p],
+    ),
+    "fsb_spmm_csr_diag": (
+        ctypes.c_int,
+        [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,
+         ctypes.c_int, ctypes.c_int, ctypes.c_int64, ctypes.c_void_p],
     ),
     "fsb_spmv_csr_noalloc": (
         ctypes.c_int,
@@ -310,9 +316,12 @@ def check(status, what):
 
 def stream_handle(device):
     """torch's current stream on ``device`` as a cudaStream_t."""
-    idx = device.index if isinstance(device, torch.device) else device
-    if idx is None:
-        idx = torch.cuda.current_device()
+    if isinstance(device, int):
+        idx = device
+    else:
+        idx = torch.device(device).index
+        if idx is None:
+            idx = torch.cuda.current_device()
     return ctypes.c_void_p(torch._C._cuda_getCurrentRawStream(idx))
 
 

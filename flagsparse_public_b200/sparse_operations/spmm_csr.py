@@ -449,7 +449,8 @@ def _triton_spmm_csr_impl(data, indices, indptr, B, n_rows, n_dense_cols, block_
     return C
 
 
-def _triton_spmm_csr_impl_opt_prepared(prepared, B, out=None):
+def _check_opt_operand(prepared, B):
+    """FlagSparse's checks of the opt paths' dense operand (``spmm_csr.py:1998-2011``)."""
     if not prepared.supports_opt:
         raise TypeError("spmm opt only supports float32 and float64")
     if not B.is_cuda:
@@ -462,7 +463,11 @@ def _triton_spmm_csr_impl_opt_prepared(prepared, B, out=None):
         raise ValueError(f"B.shape[0] must be n_cols={prepared.n_cols}, got {B.shape[0]}")
     if B.ndim != 2:
         raise ValueError("B must be a 2D dense tensor")
-    B = B.contiguous()
+    return B.contiguous()
+
+
+def _triton_spmm_csr_impl_opt_prepared(prepared, B, out=None):
+    B = _check_opt_operand(prepared, B)
     n_dense = int(B.shape[1])
     C = out if out is not None else torch.empty((prepared.n_rows, n_dense), dtype=B.dtype, device=B.device)
     if prepared.n_rows == 0 or n_dense == 0:
@@ -471,6 +476,62 @@ def _triton_spmm_csr_impl_opt_prepared(prepared, B, out=None):
     _plan.run_spmm(prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
                    prepared.n_cols, B, C, _nat.ACC_NATIVE, plan)
     return C, False
+
+
+# Diagnose-only forms (FlagSparse ``spmm_csr.py:1998-2086``): fixed-order
+# accumulation in fsb_spmm_csr_diag, for comparing the opt path's rounding
+# with float64 and compensated sums.  Rows of at most this many nonzeros take
+# the candidate form's compensated short-row arithmetic (FlagSparse
+# ``_candidate_bucket_uses_stable_short_kernel``, ``:1871-1874``).
+_DIAG_CANDIDATE_SHORT_MAX = 256
+
+
+def _run_spmm_diag(prepared, B, mode_short, mode_long, short_max):
+    B = _check_opt_operand(prepared, B)
+    n_dense = int(B.shape[1])
+    C = torch.zeros((prepared.n_rows, n_dense), dtype=B.dtype, device=B.device)
+    if prepared.n_rows == 0 or n_dense == 0:
+        return C
+    cm = _nat.make_csr(prepared.data, prepared.kernel_indices, prepared.kernel_indptr, prepared.n_rows,
+                       prepared.n_cols)
+    rc = _nat.library().fsb_spmm_csr_diag(cm, _nat.ptr(B), int(B.stride(0)), n_dense, _nat.ptr(C), int(C.stride(0)),
+                                          int(mode_short), int(mode_long), int(short_max),
+                                          _nat.stream_handle(B.device))
+    _nat.check(rc, "fsb_spmm_csr_diag")
+    _plan.LAUNCHES["count"] += 1
+    return C
+
+
+def _triton_spmm_csr_impl_opt_prepared_stable(prepared, B):
+    """The stable form: every element accumulated in float64 in nonzero order
+    and stored in the value type (FlagSparse ``:2059-2081``, its
+    ``_spmm_csr_stable_vector_*`` kernels, ``:1023-1106``)."""
+    return _run_spmm_diag(prepared, B, _nat.DIAG_WIDE, _nat.DIAG_WIDE, -1), False
+
+
+def _flagsparse_spmm_csr_opt_stable_for_diagnose(prepared, B):
+    C_out, _ = _triton_spmm_csr_impl_opt_prepared_stable(prepared, B)
+    return C_out
+
+
+def _triton_spmm_csr_impl_opt_prepared_candidate(prepared, B):
+    """The candidate form: rows of at most 256 nonzeros with Kahan's sum in
+    float64 (FlagSparse's ``_spmm_csr_candidate_stable_short_*`` kernels,
+    ``:1540-1634``), longer rows accumulated in the value precision in order."""
+    C = _run_spmm_diag(prepared, B, _nat.DIAG_KAHAN_WIDE, _nat.DIAG_NATIVE, _DIAG_CANDIDATE_SHORT_MAX)
+    return C, False
+
+
+def _flagsparse_spmm_csr_opt_candidate_for_diagnose(prepared, B):
+    C_out, _ = _triton_spmm_csr_impl_opt_prepared_candidate(prepared, B)
+    return C_out
+
+
+def _flagsparse_spmm_csr_opt_kahan_for_diagnose(prepared, B):
+    """Kahan's compensated sum in the value precision on every row (the
+    arithmetic of FlagSparse's ``_spmm_csr_stable_batched_*`` kernels,
+    ``:923-1020``)."""
+    return _run_spmm_diag(prepared, B, _nat.DIAG_KAHAN, _nat.DIAG_KAHAN, -1)
 
 
 def flagsparse_spmm_csr(

@@ -424,6 +424,29 @@ int fsb_sddmm_csr(const void* col_idx, int index_dtype, const int32_t* row_ids,
                   const void* data, void* out, int value_dtype, double alpha,
                   double beta, void* stream);
 
+/* ---- diagnostic SpMM forms ------------------------------------------ *
+ * C = A B with a fixed-order, explicitly rounded accumulation per element,
+ * the arithmetic of FlagSparse's diagnose-only SpMM paths (stable kernels
+ * spmm_csr.py:922-1249, candidate short-row kernels :1501-1634, entry
+ * points :1998-2086).  Each output element walks its row's nonzeros in
+ * order:
+ *   FSB_DIAG_NATIVE      acc = fma(a, b, acc), value precision
+ *   FSB_DIAG_WIDE        acc = fma(a, b, acc) in float64, stored in the
+ *                        value type (float64 accumulate, float32 store)
+ *   FSB_DIAG_KAHAN       y = fma(a, b, -comp); t = acc + y;
+ *                        comp = (t - acc) - y; acc = t, value precision
+ *   FSB_DIAG_KAHAN_WIDE  the same in float64, stored in the value type
+ * Rows of at most short_max nonzeros use mode_short, the others mode_long.
+ * float32 / float64 values; B (ldb) and C (ldc) row-major, C in the value
+ * type.  For diagnosis, not speed: one warp per row.                      */
+#define FSB_DIAG_NATIVE     0
+#define FSB_DIAG_WIDE       1
+#define FSB_DIAG_KAHAN      2
+#define FSB_DIAG_KAHAN_WIDE 3
+int fsb_spmm_csr_diag(const fsb_csr* A, const void* B, int64_t ldb,
+                      int64_t n_dense, void* C, int64_t ldc, int mode_short,
+                      int mode_long, int64_t short_max, void* stream);
+
 /* ---- Matrix Market ingest (host) ------------------------------------- *
  * Parses a .mtx coordinate file into CSR (float64 values, int64 indices and
  * row offsets, columns sorted in each row) with the semantics of FlagSparse's

@@ -34,6 +34,9 @@
  *                         out[p] = alpha * dot(x[row(p)], y[col(p)]) +
  *                         beta * data[p], the dot product accumulated in the
  *                         value precision (float32 / float64) in K order.
+ *   orc_spmm_diag       : the diagnose-only stable / candidate SpMM arithmetic
+ *                         (spmm_csr.py:922-1249, :1501-1634): fixed-order
+ *                         float64 or Kahan accumulation per element.
  *   orc_merge_partition : restatement of the merge-path partition kernel
  *                         (Merrill & Garland's merge-path search over row ends
  *                         and nonzero indices).
@@ -319,6 +322,71 @@ int orc_spmm_csr(const void* val, const void* col, const void* ptr, int vdt, int
         for (int64_t c = 0; c < n_dense; ++c) {
             orc_c a = dot_row(val, vdt, col, idt, s, e, B, ldb, c, prec);
             st_val(C, out_dtype, r * ldc + c, a.re, a.im);
+        }
+    }
+    return 0;
+}
+
+/* -------------------------------------------- diagnostic SpMM forms -- */
+/* FlagSparse's diagnose-only SpMM arithmetic (spmm_csr.py:922-1249 stable
+ * kernels, :1501-1634 candidate short-row kernels), per output element in
+ * nonzero order: mode 0 acc = fma(a, b, acc) in the value precision; 1 the
+ * same in double, stored in the value type; 2 Kahan in the value precision
+ * (y = fma(a, b, -comp); t = acc + y; comp = (t - acc) - y; acc = t); 3 Kahan
+ * in double.  Rows of at most short_max nonzeros use mode_short.  The
+ * fused multiply-adds are written out (fma / fmaf) and the file is built
+ * with -ffp-contract=off, so every operation is rounded where written. */
+static double diag_dot_d(const void* val, int vdt, const void* col, int idt, int64_t s, int64_t e, const void* B,
+                         int64_t ldb, int64_t n, int kahan) {
+    double acc = 0.0, comp = 0.0;
+    for (int64_t k = s; k < e; ++k) {
+        const double a = ld_re(val, vdt, k), b = ld_re(B, vdt, ld_idx(col, idt, k) * ldb + n);
+        if (kahan) {
+            const double y = fma(a, b, -comp), t = acc + y;
+            comp = (t - acc) - y;
+            acc = t;
+        } else {
+            acc = fma(a, b, acc);
+        }
+    }
+    return acc;
+}
+
+static float diag_dot_f(const float* val, const void* col, int idt, int64_t s, int64_t e, const float* B,
+                        int64_t ldb, int64_t n, int kahan) {
+    float acc = 0.f, comp = 0.f;
+    for (int64_t k = s; k < e; ++k) {
+        const float a = val[k], b = B[ld_idx(col, idt, k) * ldb + n];
+        if (kahan) {
+            const float y = fmaf(a, b, -comp), t = acc + y;
+            comp = (t - acc) - y;
+            acc = t;
+        } else {
+            acc = fmaf(a, b, acc);
+        }
+    }
+    return acc;
+}
+
+int orc_spmm_diag(const void* val, const void* col, const void* ptr, int vdt, int idt, int pdt, int64_t n_rows,
+                  const void* B, int64_t ldb, int64_t n_dense, void* C, int64_t ldc, int mode_short, int mode_long,
+                  int64_t short_max, int threads) {
+    if (vdt != ORC_F32 && vdt != ORC_F64) return -1;
+    if (threads < 1) threads = 1;
+#pragma omp parallel for schedule(dynamic, 64) num_threads(threads)
+    for (int64_t r = 0; r < n_rows; ++r) {
+        const int64_t s = ld_idx(ptr, pdt, r), e = ld_idx(ptr, pdt, r + 1);
+        const int mode = (e - s) <= short_max ? mode_short : mode_long;
+        const int kahan = mode == 2 || mode == 3;
+        for (int64_t n = 0; n < n_dense; ++n) {
+            if (vdt == ORC_F64 || mode == 1 || mode == 3) {
+                const double v = diag_dot_d(val, vdt, col, idt, s, e, B, ldb, n, kahan);
+                if (vdt == ORC_F64) ((double*)C)[r * ldc + n] = v;
+                else ((float*)C)[r * ldc + n] = (float)v;
+            } else {
+                ((float*)C)[r * ldc + n] =
+                    diag_dot_f((const float*)val, col, idt, s, e, (const float*)B, ldb, n, kahan);
+            }
         }
     }
     return 0;

@@ -53,6 +53,7 @@ def _load():
         lib.orc_split_metadata.argtypes = [vp, vp, i64, i64, vp, vp, vp, vp]
         lib.orc_split_metadata.restype = i64
         lib.orc_merge_partition.argtypes = [vp, i32, i64, i64, i64, i64, i64, vp]
+        lib.orc_spmm_diag.argtypes = [vp, vp, vp, i32, i32, i32, i64, vp, i64, i64, vp, i64, i32, i32, i64, i32]
         lib.orc_merge_runs.argtypes = [vp, i32, i64, vp, i64, vp]
         lib.orc_sddmm_csr.argtypes = [vp, i32, vp, i32, i64, vp, i64, vp, i64, i64, vp, vp, i32,
                                       ctypes.c_double, ctypes.c_double, i32]
@@ -94,6 +95,25 @@ def spmm_csr(data, indices, indptr, B, acc_mode=ACC_WIDE, out_dtype=None, thread
     _load().orc_spmm_csr(_p(data), _p(indices), _p(indptr), _CODES[data.dtype], _CODES[indices.dtype],
                          _CODES[indptr.dtype], n_rows, _p(B), B.stride(0) if B.numel() else n_dense, n_dense, _p(C),
                          n_dense, _CODES[out_dtype], acc_mode, _threads(threads))
+    return C
+
+
+def spmm_diag(data, indices, indptr, B, mode_short, mode_long=None, short_max=-1, threads=None):
+    """Diagnose-only SpMM arithmetic (orc_spmm_diag): modes 0 native fma,
+    1 float64 fma stored in the value type, 2 Kahan, 3 Kahan in float64; rows
+    of at most ``short_max`` nonzeros use ``mode_short``, the others
+    ``mode_long`` (default: the same)."""
+    data, indices, indptr, B = map(_host, (data, indices, indptr, B))
+    B = B.contiguous()
+    n_rows = indptr.numel() - 1
+    n_dense = B.shape[1]
+    mode_long = mode_short if mode_long is None else mode_long
+    C = torch.empty((n_rows, n_dense), dtype=data.dtype)
+    rc = _load().orc_spmm_diag(_p(data), _p(indices), _p(indptr), _CODES[data.dtype], _CODES[indices.dtype],
+                               _CODES[indptr.dtype], n_rows, _p(B), n_dense, n_dense, _p(C), n_dense, int(mode_short),
+                               int(mode_long), int(short_max), _threads(threads))
+    if rc != 0:
+        raise TypeError("orc_spmm_diag: float32 / float64 values only")
     return C
 
 
