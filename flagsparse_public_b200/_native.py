@@ -152,6 +152,11 @@ _SIGNATURES = {
         [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_void_p,
          ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(FsbPlan), ctypes.c_void_p],
     ),
+    "fsb_coo_coalesce": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_int64,
+         ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p],
+    ),
     "fsb_spmm_csr_diag": (
         ctypes.c_int,
         [ctypes.POINTER(FsbCsr), ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64,

@@ -351,6 +351,41 @@ def stable_sort(keys, key_bound=None):
     return out, order
 
 
+def run_starts_device(sorted_keys, out_dtype):
+    """fsb_run_starts without a host read: (starts buffer of n + 1 entries,
+    device int64 tensor holding how many of them were written)."""
+    keys = sorted_keys.contiguous()
+    n = keys.numel()
+    lib = nat.library()
+    starts = torch.empty(n + 1, dtype=out_dtype, device=keys.device)
+    count = torch.zeros(1, dtype=torch.int64, device=keys.device)
+    if n == 0:
+        return starts, count
+    nbytes = int(lib.fsb_run_starts_workspace_bytes(n))
+    ws = torch.empty(nbytes, dtype=torch.uint8, device=keys.device)
+    rc = lib.fsb_run_starts(nat.ptr(keys), nat.dtype_code(keys.dtype), n, nat.ptr(starts), nat.dtype_code(out_dtype),
+                            nat.ptr(count), nat.ptr(ws), nbytes, nat.stream_handle(keys.device))
+    nat.check(rc, "fsb_run_starts")
+    return starts, count
+
+
+def coalesce_sorted(sorted_keys, order, values):
+    """Distinct keys and their summed values (fsb_coo_coalesce) of stably
+    sorted keys; buffers of n entries and the device count of distinct keys
+    (no host read)."""
+    n = sorted_keys.numel()
+    out_keys = torch.empty_like(sorted_keys)
+    out_vals = torch.empty_like(values)
+    starts, count = run_starts_device(sorted_keys, torch.int64)
+    if n:
+        rc = nat.library().fsb_coo_coalesce(nat.ptr(sorted_keys), nat.dtype_code(sorted_keys.dtype), nat.ptr(order),
+                                            nat.ptr(values), nat.dtype_code(values.dtype), n, nat.ptr(starts),
+                                            nat.dtype_code(starts.dtype), nat.ptr(count), nat.ptr(out_keys),
+                                            nat.ptr(out_vals), nat.stream_handle(values.device))
+        nat.check(rc, "fsb_coo_coalesce")
+    return out_keys, out_vals, (count - 1).clamp_(min=0)
+
+
 def run_starts(sorted_keys, out_dtype):
     """[0, start of every later run of equal keys ..., n] of sorted 1-D keys in
     ``out_dtype`` (int32 / int64): fsb_run_starts on CUDA tensors (one host
@@ -364,16 +399,7 @@ def run_starts(sorted_keys, out_dtype):
         breaks = torch.nonzero(sorted_keys[1:] != sorted_keys[:-1], as_tuple=False).flatten().to(out_dtype) + 1
         return torch.cat([torch.zeros(1, dtype=out_dtype, device=dev), breaks,
                           torch.tensor([n], dtype=out_dtype, device=dev)])
-    keys = sorted_keys.contiguous()
-    lib = nat.library()
-    starts = torch.empty(n + 1, dtype=out_dtype, device=keys.device)
-    count = torch.empty(1, dtype=torch.int64, device=keys.device)
-    nbytes = int(lib.fsb_run_starts_workspace_bytes(n))
-    ws = torch.empty(nbytes, dtype=torch.uint8, device=keys.device)
-    rc = lib.fsb_run_starts(nat.ptr(keys), nat.dtype_code(keys.dtype), n, nat.ptr(starts),
-                            nat.dtype_code(out_dtype), nat.ptr(count), nat.ptr(ws), nbytes,
-                            nat.stream_handle(keys.device))
-    nat.check(rc, "fsb_run_starts")
+    starts, count = run_starts_device(sorted_keys, out_dtype)
     return starts[: int(count.item())].clone()
 
 

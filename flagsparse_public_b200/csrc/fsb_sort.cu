@@ -26,6 +26,8 @@
 // int64 by the last pass.  Keys of the full signed width are ordered through
 // their top bit flipped.  HBM bound: a pass reads the keys twice and the
 // permutation once and writes both.
+#include <algorithm>
+
 #include "fsb_dispatch.cuh"
 
 namespace fsb {
@@ -242,6 +244,82 @@ k_run_write(const K* __restrict__ keys, int64_t n, const uint32_t* __restrict__ 
     }
 }
 
+// Duplicate merge of sorted COO entries (torch's coalesce, which FlagSparse
+// calls in _coalesce_coo_entries, spmm_coo.py:35-51): one thread per run of
+// equal keys sums its values in sorted (= original, the sort is stable)
+// order, starting from zero in the accumulation type -- float for half types
+// and float32, double for float64, float / double pairs for complex -- and
+// rounds once to the value type.  Fewer than two entries are copied as they
+// are.  The run count is read on the device, so nothing returns to the host.
+template <class V> struct CoalesceAcc;
+template <> struct CoalesceAcc<float> {
+    using A = float;
+    static __device__ __forceinline__ A zero() { return 0.f; }
+    static __device__ __forceinline__ A add(A a, float v) { return __fadd_rn(a, v); }
+    static __device__ __forceinline__ float out(A a) { return a; }
+};
+template <> struct CoalesceAcc<double> {
+    using A = double;
+    static __device__ __forceinline__ A zero() { return 0.0; }
+    static __device__ __forceinline__ A add(A a, double v) { return __dadd_rn(a, v); }
+    static __device__ __forceinline__ double out(A a) { return a; }
+};
+template <> struct CoalesceAcc<__half> {
+    using A = float;
+    static __device__ __forceinline__ A zero() { return 0.f; }
+    static __device__ __forceinline__ A add(A a, __half v) { return __fadd_rn(a, __half2float(v)); }
+    static __device__ __forceinline__ __half out(A a) { return __float2half_rn(a); }
+};
+template <> struct CoalesceAcc<__nv_bfloat16> {
+    using A = float;
+    static __device__ __forceinline__ A zero() { return 0.f; }
+    static __device__ __forceinline__ A add(A a, __nv_bfloat16 v) { return __fadd_rn(a, __bfloat162float(v)); }
+    static __device__ __forceinline__ __nv_bfloat16 out(A a) { return __float2bfloat16_rn(a); }
+};
+template <> struct CoalesceAcc<c64_t> {
+    using A = c64_t;
+    static __device__ __forceinline__ A zero() { return c64_t{0.f, 0.f}; }
+    static __device__ __forceinline__ A add(A a, c64_t v) { return c64_t{__fadd_rn(a.re, v.re), __fadd_rn(a.im, v.im)}; }
+    static __device__ __forceinline__ c64_t out(A a) { return a; }
+};
+template <> struct CoalesceAcc<c128_t> {
+    using A = c128_t;
+    static __device__ __forceinline__ A zero() { return c128_t{0.0, 0.0}; }
+    static __device__ __forceinline__ A add(A a, c128_t v) {
+        return c128_t{__dadd_rn(a.re, v.re), __dadd_rn(a.im, v.im)};
+    }
+    static __device__ __forceinline__ c128_t out(A a) { return a; }
+};
+template <> struct CoalesceAcc<c32_t> {
+    using A = c64_t;
+    static __device__ __forceinline__ A zero() { return c64_t{0.f, 0.f}; }
+    static __device__ __forceinline__ A add(A a, c32_t v) {
+        return c64_t{__fadd_rn(a.re, __half2float(v.re)), __fadd_rn(a.im, __half2float(v.im))};
+    }
+    static __device__ __forceinline__ c32_t out(A a) { return c32_t{__float2half_rn(a.re), __float2half_rn(a.im)}; }
+};
+
+template <class V, class K, class O>
+__global__ void __launch_bounds__(kThreads)
+k_coo_segment_sum(const K* __restrict__ keys, const O* __restrict__ starts, const int64_t* __restrict__ count,
+                  const int64_t* __restrict__ order, const V* __restrict__ vals, int64_t n, K* __restrict__ out_keys,
+                  V* __restrict__ out_vals) {
+    using C = CoalesceAcc<V>;
+    const int64_t runs = *count - 1;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t j = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; j < runs; j += stride) {
+        const int64_t s = (int64_t)starts[j], e = (int64_t)starts[j + 1];
+        out_keys[j] = keys[s];
+        if (n < 2) {
+            out_vals[j] = vals[order[s]];
+            continue;
+        }
+        typename C::A acc = C::zero();
+        for (int64_t k = s; k < e; ++k) acc = C::add(acc, vals[order[k]]);
+        out_vals[j] = C::out(acc);
+    }
+}
+
 // Dynamic shared memory of k_sort_downsweep: the staged keys and permutation.
 template <class K>
 constexpr int downsweep_smem() {
@@ -420,4 +498,48 @@ extern "C" int fsb_run_starts(const void* sorted_keys, int key_dtype, int64_t n,
     }
     if (starts_dtype == FSB_I32) return go(tag<int64_t>{}, tag<int32_t>{});
     return go(tag<int64_t>{}, tag<int64_t>{});
+}
+
+extern "C" int fsb_coo_coalesce(const void* sorted_keys, int key_dtype, const int64_t* order, const void* values,
+                                int value_dtype, int64_t n, const void* starts, int starts_dtype, const int64_t* count,
+                                void* out_keys, void* out_values, void* stream) {
+    if (n < 0 || (key_dtype != FSB_I32 && key_dtype != FSB_I64) ||
+        (starts_dtype != FSB_I32 && starts_dtype != FSB_I64)) {
+        fsb_host::set_error("fsb_coo_coalesce: bad sizes or index dtypes");
+        return FSB_ERR_INVALID;
+    }
+    if (n == 0) return FSB_OK;
+    if (!sorted_keys || !order || !values || !starts || !count || !out_keys || !out_values) {
+        fsb_host::set_error("fsb_coo_coalesce: null pointer");
+        return FSB_ERR_INVALID;
+    }
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int64_t blocks = std::min<int64_t>(ceil_div(n, (int64_t)sort::kThreads), 148 * 16);
+    auto go = [&](auto tv) -> int {
+        using V = typename decltype(tv)::type;
+        auto go2 = [&](auto tk, auto to) -> int {
+            using K = typename decltype(tk)::type;
+            using O = typename decltype(to)::type;
+            sort::k_coo_segment_sum<V, K, O><<<(unsigned)blocks, sort::kThreads, 0, st>>>(
+                static_cast<const K*>(sorted_keys), static_cast<const O*>(starts), count, order,
+                static_cast<const V*>(values), n, static_cast<K*>(out_keys), static_cast<V*>(out_values));
+            return fsb_host::check_launch("k_coo_segment_sum");
+        };
+        if (key_dtype == FSB_I32) {
+            return starts_dtype == FSB_I32 ? go2(tag<int32_t>{}, tag<int32_t>{}) : go2(tag<int32_t>{}, tag<int64_t>{});
+        }
+        return starts_dtype == FSB_I32 ? go2(tag<int64_t>{}, tag<int32_t>{}) : go2(tag<int64_t>{}, tag<int64_t>{});
+    };
+    switch (value_dtype) {
+    case FSB_F16: return go(tag<__half>{});
+    case FSB_BF16: return go(tag<__nv_bfloat16>{});
+    case FSB_F32: return go(tag<float>{});
+    case FSB_F64: return go(tag<double>{});
+    case FSB_C64: return go(tag<c64_t>{});
+    case FSB_C128: return go(tag<c128_t>{});
+    case FSB_C32: return go(tag<c32_t>{});
+    default:
+        fsb_host::set_error("fsb_coo_coalesce: unsupported value dtype %d", value_dtype);
+        return FSB_ERR_UNSUPPORTED;
+    }
 }

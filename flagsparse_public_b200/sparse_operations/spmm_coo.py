@@ -47,12 +47,32 @@ def _sort_coo_lex_inplace(data, row, col, n_cols, n_rows=None):
     return data[order].contiguous(), row64[order].contiguous(), col64[order].contiguous()
 
 
+def _coalesce_coo_device(data, row, col, shape):
+    """Duplicate merge on the device without a host read: the (row, col) keys
+    stably sorted (fsb_stable_sort), runs of equal keys (fsb_run_starts) and
+    their values summed in sorted order (fsb_coo_coalesce).  Returns buffers
+    of nnz entries (values, int64 rows, int64 cols) and the device count of
+    distinct entries; safe to record in a CUDA graph."""
+    n_rows, n_cols = int(shape[0]), int(shape[1])
+    key = row.to(torch.int64) * max(1, n_cols) + col.to(torch.int64)
+    sorted_key, order = _plan.stable_sort(key, key_bound=max(1, n_rows) * max(1, n_cols))
+    ukeys, uvals, count = _plan.coalesce_sorted(sorted_key, order, data.contiguous())
+    return uvals, ukeys // max(1, n_cols), ukeys % max(1, n_cols), count
+
+
 def _coalesce_coo_entries(data, row, col, shape):
-    """Merge duplicate (row, col) entries by summing values (FlagSparse ``spmm_coo.py:35-51``)."""
+    """Merge duplicate (row, col) entries by summing values (FlagSparse ``spmm_coo.py:35-51``,
+    which calls torch's coalesce): on CUDA tensors the device merge above,
+    equal to torch's coalesce bit for bit, with one host read of the count;
+    host tensors (the reference's own fixtures) go through torch."""
     n_rows, n_cols = int(shape[0]), int(shape[1])
     if data.numel() == 0:
         z = torch.empty(0, dtype=torch.int64, device=data.device)
         return data.contiguous(), z, z.clone()
+    if data.is_cuda:
+        vals, rows, cols, count = _coalesce_coo_device(data, row, col, shape)
+        m = int(count.item())
+        return vals[:m].contiguous(), rows[:m].contiguous(), cols[:m].contiguous()
     coo = torch.sparse_coo_tensor(torch.stack([row.to(torch.int64), col.to(torch.int64)]), data,
                                   size=(n_rows, n_cols), device=data.device, dtype=data.dtype).coalesce()
     idx = coo.indices()
@@ -95,7 +115,9 @@ def _prepare_spmm_coo_inputs(data, row, col, B, shape):
     nnz = data.numel()
     if nnz > _INDEX_LIMIT_INT32:
         raise ValueError("nnz exceeds the int32 range supported by the Triton COO kernel")
-    if nnz > 0:
+    # the index checks read the device: skipped while a CUDA graph records
+    # the call (the caller checks the indices before capturing)
+    if nnz > 0 and not torch.cuda.is_current_stream_capturing():
         lim = torch.stack([row.min().to(torch.int64), row.max().to(torch.int64), col.min().to(torch.int64),
                            col.max().to(torch.int64)]).tolist()
         min_row, max_row, min_col, max_col = lim
@@ -174,7 +196,10 @@ def _triton_spmm_coo_impl(data, row, col, B, n_rows, n_dense_cols, block_n, bloc
     if route == "rowrun":
         d, c, indptr = _coo_rows_to_csr(data, row, col, n_rows)
         C = torch.empty((n_rows, n_dense_cols), dtype=data.dtype, device=device)
-        stats = _plan.matrix_stats(indptr, n_rows, B.shape[0])
+        # the merge-path plan needs only the sizes the host knows (rows +
+        # nonzeros per unit): no statistics read from the device
+        nnz = data.numel()
+        stats = _plan.MatrixStats(n_rows, B.shape[0], nnz, nnz, nnz / max(n_rows, 1), 0.0, 0)
         plan = _plan.default_spmm_plan(stats, n_dense_cols, data.dtype)
         _plan.run_spmm(d, c, indptr, n_rows, B.shape[0], B, C, _acc_mode_for(data.dtype), plan)
         return C if C.dtype == out_dtype else C.to(out_dtype)

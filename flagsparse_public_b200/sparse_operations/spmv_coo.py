@@ -4,9 +4,10 @@ Follows FlagSparse ``sparse_operations/spmv_coo.py``:
 
 - ``sort_by_row=True`` (default): lexicographic (row, col) sort and row-run
   offsets ``seg_starts`` (length #runs + 1, ``spmv_coo.py:297-327``); one
-  result per run, no atomics.  Here the runs go through the CSR kernels of
-  ``libflagsparse_b200.so`` with ``row_ptr = seg_starts`` and the sorted row
-  array as the output-row map.
+  result per run, no atomics.  Here the sort, the run bounds and the row
+  offsets stay on the device (the run bounds reach the host only when
+  ``seg_starts`` is read) and the runs go through the CSR kernels of
+  ``libflagsparse_b200.so`` as rows of the sorted structure.
 - ``sort_by_row=False``: one atomic add per nonzero (``:229-294``).
 
 Accumulation is in the value precision (float32 for float32, ``:148``).
@@ -62,7 +63,13 @@ def _normalize_spmv_coo_index_fallback_policy(index_fallback_policy):
 
 
 class PreparedCoo:
-    """Sorted COO + optional row-run bounds ``seg_starts`` (FlagSparse ``spmv_coo.py:77-128``)."""
+    """Sorted COO + optional row-run bounds ``seg_starts`` (FlagSparse ``spmv_coo.py:77-128``).
+
+    ``seg_starts`` may be given as a tensor (FlagSparse's constructor) or, from
+    ``prepare_spmv_coo``, as ``runs`` = (starts buffer, device run count): the
+    run bounds are then read to the host only when ``seg_starts`` / ``n_segs``
+    are first accessed, so a prepare records in a CUDA graph.  The products
+    run over per-row offsets of the sorted rows, which need no run count."""
 
     __slots__ = (
         "data",
@@ -72,8 +79,9 @@ class PreparedCoo:
         "n_rows",
         "n_cols",
         "nnz",
-        "seg_starts",
-        "n_segs",
+        "_seg_starts",
+        "_runs",
+        "_row_ptr",
         "use_seg_kernel",
         "op",
         "transpose",
@@ -95,6 +103,7 @@ class PreparedCoo:
         index_fallback_policy="auto",
         index_fallback_applied=False,
         index_fallback_reason=None,
+        runs=None,
     ):
         self.data = data
         self.row = row
@@ -102,19 +111,32 @@ class PreparedCoo:
         self.shape = (int(shape[0]), int(shape[1]))
         self.n_rows, self.n_cols = self.shape
         self.nnz = int(data.numel())
-        self.seg_starts = seg_starts
-        if seg_starts is None:
-            self.n_segs = 0
-            self.use_seg_kernel = False
+        self._seg_starts = seg_starts
+        self._runs = runs if seg_starts is None else None
+        self._row_ptr = None
+        if seg_starts is not None:
+            self.use_seg_kernel = int(seg_starts.numel()) - 1 > 0
         else:
-            self.n_segs = int(seg_starts.numel()) - 1
-            self.use_seg_kernel = self.n_segs > 0
+            self.use_seg_kernel = self._runs is not None and self.nnz > 0
         self.op = _normalize_spmv_coo_op(op, transpose=transpose)
         self.transpose = _spmv_coo_op_transposes(self.op)
         self.index_fallback_policy = str(index_fallback_policy).lower()
         self.index_fallback_applied = bool(index_fallback_applied)
         self.index_fallback_reason = index_fallback_reason
         self._plan = None
+
+    @property
+    def seg_starts(self):
+        if self._seg_starts is None and self._runs is not None:
+            starts, count = self._runs
+            self._seg_starts = starts[: int(count.item())].clone()
+            self._runs = None
+        return self._seg_starts
+
+    @property
+    def n_segs(self):
+        seg = self.seg_starts
+        return 0 if seg is None else int(seg.numel()) - 1
 
 
 def _sort_coo_lex_inplace(data, row, col, n_cols, n_rows=None):
@@ -156,20 +178,23 @@ def _prepare_coo_tensors(data, row, col, shape, sort_by_row):
     index_dtype = torch.promote_types(row.dtype, col.dtype)
     if sort_by_row:
         data, kr, kc = _sort_coo_lex_inplace(data, row, col, n_cols, n_rows)
-        seg = _seg_starts_from_sorted_rows(kr, data.numel(), data.device)
+        nnz = data.numel()
+        runs = _plan.run_starts_device(kr, kr.dtype if nnz <= _INDEX_LIMIT_INT32 else torch.int64) if nnz else None
     else:
         data = data.contiguous()
         kr = row.to(index_dtype).contiguous()
         kc = col.to(index_dtype).contiguous()
-        seg = None
-    if data.numel() > 0:
+        runs = None
+    # the index checks read the device: skipped while a CUDA graph records
+    # the prepare (the caller checks the indices before capturing)
+    if data.numel() > 0 and not torch.cuda.is_current_stream_capturing():
         lim = torch.stack([kr.min().to(torch.int64), kr.max().to(torch.int64),
                            kc.min().to(torch.int64), kc.max().to(torch.int64)]).tolist()
         if lim[0] < 0 or lim[1] >= n_rows:
             raise IndexError("row indices out of range")
         if lim[2] < 0 or lim[3] >= n_cols:
             raise IndexError("col indices out of range")
-    return data, kr, kc, seg
+    return data, kr, kc, runs
 
 
 def prepare_spmv_coo(data, row, col, shape, sort_by_row=True, transpose=False, op=None,
@@ -185,9 +210,13 @@ def prepare_spmv_coo(data, row, col, shape, sort_by_row=True, transpose=False, o
         row, col = col, row
         if op_code == SPMV_COO_OP_CONJ_TRANS and _is_complex_dtype(data.dtype):
             data = data.conj().resolve_conj()
-    d, kr, kc, seg = _prepare_coo_tensors(data, row, col, shape, sort_by_row)
-    return PreparedCoo(d, kr, kc, shape, seg_starts=seg, transpose=transpose, op=op_code,
-                       index_fallback_policy=index_fallback_policy)
+    d, kr, kc, runs = _prepare_coo_tensors(data, row, col, shape, sort_by_row)
+    if sort_by_row and runs is None:  # no entries: the one-entry run bound of FlagSparse
+        seg = torch.zeros(1, dtype=kr.dtype, device=d.device)
+        return PreparedCoo(d, kr, kc, shape, seg_starts=seg, transpose=transpose, op=op_code,
+                           index_fallback_policy=index_fallback_policy)
+    return PreparedCoo(d, kr, kc, shape, transpose=transpose, op=op_code, index_fallback_policy=index_fallback_policy,
+                       runs=runs)
 
 
 def _validate_x_coo(x, prepared):
@@ -206,9 +235,21 @@ def _validate_x_coo(x, prepared):
     return x.contiguous()
 
 
+def _coo_row_ptr(prepared):
+    """int64 offsets of the sorted rows (fsb_sorted_keys_to_offsets): every
+    row, empty ones included, so no run count is needed on the host."""
+    if prepared._row_ptr is None:
+        prepared._row_ptr = _plan.sorted_keys_to_offsets(prepared.row, prepared.n_rows)
+    return prepared._row_ptr
+
+
 def _coo_run_plan(prepared):
+    """Plan from the sizes the host knows: the longest row is taken as
+    unknown (as long as all nonzeros), so short-row matrices go merge path,
+    which is balanced whatever the row lengths."""
     if prepared._plan is None:
-        stats = _plan.matrix_stats(prepared.seg_starts, prepared.n_segs, prepared.n_cols)
+        n, nnz = prepared.n_rows, prepared.nnz
+        stats = _plan.MatrixStats(n, prepared.n_cols, nnz, nnz, nnz / max(n, 1), 0.0, 0)
         prepared._plan = _plan.default_spmv_plan(stats, prepared.data.dtype)
     return prepared._plan
 
@@ -225,9 +266,10 @@ def _triton_spmv_coo_kernel(prepared, x, block_size, num_warps, block_inner):
     if prepared.nnz == 0:
         return y
     if prepared.use_seg_kernel:
-        row_map = prepared.row if prepared.row.dtype == prepared.col.dtype else prepared.row.to(prepared.col.dtype)
-        _plan.run_spmv(prepared.data, prepared.col, prepared.seg_starts, prepared.n_segs, prepared.n_cols, x, y,
-                       _nat.ACC_NATIVE, _coo_run_plan(prepared), row_map=row_map)
+        # the row runs as rows of a CSR structure over all rows: each run's
+        # sum in entry order, empty rows 0
+        _plan.run_spmv(prepared.data, prepared.col, _coo_row_ptr(prepared), prepared.n_rows, prepared.n_cols, x, y,
+                       _nat.ACC_NATIVE, _coo_run_plan(prepared))
         return y
     lib = _nat.library()
     row = prepared.row if prepared.row.dtype == prepared.col.dtype else prepared.row.to(prepared.col.dtype)

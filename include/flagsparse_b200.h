@@ -313,6 +313,21 @@ int fsb_run_starts(const void* sorted_keys, int key_dtype, int64_t n,
                    void* starts, int starts_dtype, int64_t* count,
                    void* workspace, int64_t workspace_bytes, void* stream);
 
+/* Duplicate merge of sorted COO entries (torch's coalesce, called by
+ * FlagSparse's _coalesce_coo_entries, spmm_coo.py:35-51): with keys sorted
+ * stably (fsb_stable_sort: sorted_keys, order) and their runs (fsb_run_starts:
+ * starts, count), out_keys[j] = the j-th distinct key and out_values[j] =
+ * the sum of its values in sorted order, from zero in float (half types,
+ * float32), double (float64) or their pairs (complex), rounded once to the
+ * value type; with n < 2 the value is copied unchanged.  out_keys /
+ * out_values need room for n entries; *count - 1 of them are written (the
+ * count stays on the device).                                             */
+int fsb_coo_coalesce(const void* sorted_keys, int key_dtype,
+                     const int64_t* order, const void* values,
+                     int value_dtype, int64_t n, const void* starts,
+                     int starts_dtype, const int64_t* count, void* out_keys,
+                     void* out_values, void* stream);
+
 /* ---- structured form: runs of consecutive columns and long rows -------- *
  * Descriptors added to a CSR matrix (which stays as it is) for the precision
  * form's SpMV / SpMM on matrices whose nonzeros sit mostly in runs of
