@@ -297,6 +297,33 @@ class SpmmPowerlaw:
                 "what": "learned selector's plan (prepared path) vs exhaustive autotuning over every candidate "
                         "plan on this matrix, same timing protocol"}
 
+    def gather_floor(self, flush, steps=20, warmup=5):
+        """The gather floor of this product: fsb_gather_floor gathers the same
+        B rows for the same column-index stream and does nothing else (every
+        variant timed with the bench protocol, the fastest kept)."""
+        from flagsparse_public_b200 import _native as nat
+
+        lib = nat.library()
+        _, indices, _ = self.A
+        sms = torch.cuda.get_device_properties(self.B.device).multi_processor_count
+        out = torch.empty(sms * 16 * 128, dtype=torch.float32, device=self.B.device)
+        stream = nat.stream_handle(self.B.device)
+        times = []
+        for variant in range(nat.GATHER_FLOOR_VARIANTS):
+            def run(variant=variant):
+                rc = lib.fsb_gather_floor(nat.ptr(indices), self.nnz, nat.ptr(self.B), int(self.B.stride(0)),
+                                          self.n_dense, nat.ptr(out), out.numel(), variant, stream)
+                nat.check(rc, "fsb_gather_floor")
+
+            times.append(_time_form(run, steps, warmup, flush, 1))
+        best = min(range(len(times)), key=times.__getitem__)
+        row_bytes = self.n_dense * 4
+        return {"ms": times[best], "variant": best, "variants_ms": times,
+                "gathered_rows_per_s": self.nnz / (times[best] * 1e-3),
+                "gathered_gbs": self.nnz * row_bytes / (times[best] * 1e-3) / 1e9,
+                "what": "fsb_gather_floor: the same B-row gathers (one 256-byte row per nonzero, same column "
+                        "stream, L2 flushed) with no other work; the product's speed limit"}
+
     # end to end through the public API from pinned host memory
     def host_inputs(self):
         data, indices, indptr = self.A
@@ -1214,7 +1241,7 @@ def parse_plan(text):
                                 n_tile=nums[2] if len(nums) > 2 else 0, flags=nat.PLAN_TMA_GATHER)
     algo = {"merge": nat.ALGO_MERGE, "flat": nat.ALGO_FLAT, "gather": nat.ALGO_GATHER, "seq": nat.ALGO_SEQ}[kind]
     return _plan.KernelPlan(algo, items_per_unit=nums[0], snap=nums[1] if len(nums) > 1 else 0,
-                            n_tile=nums[2] if len(nums) > 2 else 0)
+                            n_tile=nums[2] if len(nums) > 2 else 0, grid_blocks=nums[3] if len(nums) > 3 else 0)
 
 
 def _graph_kernels(wl):
@@ -1374,6 +1401,10 @@ def run_ours(args):
     head = measure(wl, args.workload, args, device, flush, world, rank, args.steps, args.warmup,
                    0.0 if args.no_cpu else 10.0, with_e2e=not args.no_e2e)
     selector = wl.selector_check(flush) if hasattr(wl, "selector_check") and rank == 0 and not args.only else None
+    if hasattr(wl, "gather_floor") and rank == 0:
+        floor = wl.gather_floor(flush)
+        floor["product_over_floor"] = head["ms_per_step"] / floor["ms"]
+        head["roofline"]["gather_floor"] = floor
     config = {**wl.config(), "plan": head["plan"]}
     del wl
     torch.cuda.empty_cache()

@@ -29,6 +29,7 @@ ACC_NATIVE, ACC_WIDE, ACC_COMP = 0, 1, 2
 ALGO_ROWS, ALGO_MERGE, ALGO_FLAT, ALGO_GATHER, ALGO_SEQ = 0, 1, 2, 3, 4
 PLAN_TMA_GATHER = 1  # fsb_plan.flags: SEQ with B rows staged by TMA tile::gather4
 PLAN_OVERLAP_LAUNCH = 2  # fsb_plan.flags: ROWS SpMV with programmatic dependent launch
+GATHER_FLOOR_VARIANTS = 4  # fsb_gather_floor variants (gathers in flight x resident warps)
 DIAG_NATIVE, DIAG_WIDE, DIAG_KAHAN, DIAG_KAHAN_WIDE = 0, 1, 2, 3  # fsb_spmm_csr_diag accumulations
 BSR_STAGE_TMA, BSR_STAGE_THREADS = 0, 1
 
@@ -260,6 +261,11 @@ _SIGNATURES = {
         ctypes.c_int,
         [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int, ctypes.c_float,
          ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_float, ctypes.c_void_p],
+    ),
+    "fsb_gather_floor": (
+        ctypes.c_int,
+        [ctypes.c_void_p, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64, ctypes.c_int64, ctypes.c_void_p,
+         ctypes.c_int64, ctypes.c_int, ctypes.c_void_p],
     ),
 }
 

@@ -522,6 +522,21 @@ int fsb_adam_step(float* params, const float* grad, float* m1, float* m2,
                   int n_params, float lr, float beta1, float beta2, float eps,
                   int step, float weight_decay, void* stream);
 
+/* ---- measurement: the gather floor of an SpMM ---------------------------
+ * No counterpart in FlagSparse: a roofline probe for the SpMM kernels.
+ * Gathers, for each of the nnz column indices col_idx[k] (int32, each in
+ * [0, rows of B)), the float32 row B[col_idx[k]][0 .. n_dense) (n_dense 32,
+ * 64 or 128, 16-byte aligned rows of stride ldb) exactly as the product
+ * kernels do, and adds them into per-thread sums written to out (at least
+ * SMs x 16 x 128 floats).  Nothing else is computed, so its time on a
+ * matrix is the speed limit of any product that reads one B row per
+ * nonzero.  variant in [0, FSB_GATHER_FLOOR_VARIANTS): gathers in flight per
+ * lane x resident warps (4 x 64, 8 x 32, 16 x 16, 6 x 48 per SM).          */
+#define FSB_GATHER_FLOOR_VARIANTS 4
+int fsb_gather_floor(const int32_t* col_idx, int64_t nnz, const float* B,
+                     int64_t ldb, int64_t n_dense, float* out,
+                     int64_t out_len, int variant, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

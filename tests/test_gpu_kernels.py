@@ -386,3 +386,31 @@ def test_overlapped_launch_chain_equals_plain(captured):
     overlapped = chain(nat.PLAN_OVERLAP_LAUNCH)
     assert torch.isfinite(plain).all()
     assert torch.equal(plain, overlapped)
+
+
+@pytest.mark.parametrize("n_dense", [32, 64, 128])
+def test_gather_floor_probe_gathers_every_row(n_dense):
+    """fsb_gather_floor reads each nonzero's B row once: the sum of its
+    per-thread sums equals the sum of the gathered rows (every variant)."""
+    g = torch.Generator().manual_seed(71)
+    nnz, n_cols = 100_003, 5000
+    col = torch.randint(0, n_cols, (nnz,), generator=g, dtype=torch.int32)
+    B = torch.rand((n_cols, n_dense), generator=g, dtype=torch.float64)
+    expect = float(B[col.long()].sum())
+    lib = nat.library()
+    sms = torch.cuda.get_device_properties(0).multi_processor_count
+    out = torch.empty(sms * 16 * 128, device=DEV)
+    dc, dB = col.to(DEV), B.float().to(DEV)
+    for variant in range(nat.GATHER_FLOOR_VARIANTS):
+        out.fill_(float("nan"))
+        used = out[: sms * {0: 16, 1: 8, 2: 4, 3: 12}[variant] * 128]
+        rc = lib.fsb_gather_floor(nat.ptr(dc), nnz, nat.ptr(dB), n_dense, n_dense, nat.ptr(out), out.numel(),
+                                  variant, nat.stream_handle(torch.device(DEV)))
+        nat.check(rc, "fsb_gather_floor")
+        torch.cuda.synchronize()
+        assert abs(float(used.double().sum()) - expect) <= 1e-5 * expect
+    # unsupported widths and too small an output are rejected before any launch
+    assert lib.fsb_gather_floor(nat.ptr(dc), nnz, nat.ptr(dB), 48, 48, nat.ptr(out), out.numel(), 0,
+                                nat.stream_handle(torch.device(DEV))) == nat.FSB_ERR_UNSUPPORTED
+    assert lib.fsb_gather_floor(nat.ptr(dc), nnz, nat.ptr(dB), n_dense, n_dense, nat.ptr(out), 128, 0,
+                                nat.stream_handle(torch.device(DEV))) == nat.FSB_ERR_INVALID

@@ -87,6 +87,7 @@ def test_header_constants_match_the_binding():
         "FSB_PLAN_TMA_GATHER": nat.PLAN_TMA_GATHER, "FSB_BSR_STAGE_TMA": nat.BSR_STAGE_TMA,
         "FSB_BSR_STAGE_THREADS": nat.BSR_STAGE_THREADS, "FSB_ERR_UNSUPPORTED": nat.FSB_ERR_UNSUPPORTED,
         "FSB_ERR_WORKSPACE": nat.FSB_ERR_WORKSPACE, "FSB_OK": nat.FSB_OK,
+        "FSB_GATHER_FLOOR_VARIANTS": nat.GATHER_FLOOR_VARIANTS,
     }
     for name, value in mirrored.items():
         assert defines.get(name) == value, name
