@@ -286,11 +286,14 @@ class SpmmPowerlaw:
             def run(plan=plan, C=C):
                 _plan.run_spmm(data, indices, indptr, self.shape[0], self.shape[1], self.B, C, nat.ACC_NATIVE, plan)
 
-            times[name] = _time_form(run, steps, warmup, flush, 1)
+            try:
+                times[name] = _time_form(run, steps, warmup, flush, 1)
+            except ValueError:  # a plan that cannot run these operands (BSR on float32 values)
+                times[name] = None
         chosen = _spmm_plan_for(self.prepared, "opt", self.n_dense)
         chosen_name = next((n for n, f in tuning.SPMM_CANDIDATES if f().key() == chosen.key()), None)
         chosen_ms = _time_form(self.step, steps, warmup, flush, 1)
-        best = min(times, key=times.get)
+        best = min((n for n in times if times[n] is not None), key=times.get)
         return {"mode": _plan.plan_selector(), "chosen": chosen_name or chosen.describe(), "chosen_ms": chosen_ms,
                 "autotune_best": best, "autotune_best_ms": times[best], "regret": chosen_ms / times[best],
                 "candidates_ms": times,

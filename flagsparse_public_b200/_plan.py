@@ -29,7 +29,7 @@ LAUNCHES = {"count": 0}
 
 
 def _kernels_per_call(plan):
-    if plan.algo == nat.ALGO_ROWS:
+    if plan.algo == nat.ALGO_ROWS or plan.algo == ALGO_BSR:
         return 1
     return 1 if plan.in_kernel_finish() else 2
 
@@ -177,6 +177,79 @@ class KernelPlan:
                              coords=self.coords, n_units=self.n_units, row_cap=self.row_cap,
                              comp_threshold=self.comp_threshold, grid_blocks=self.grid_blocks, flags=self.flags,
                              runs=self.runs if finish else None, tickets=self.tickets if finish else None)
+
+
+# Plan kind (host side only) of the tensor-core BSR candidate.
+ALGO_BSR = -1
+# Largest fill-in the BSR candidate accepts: stored block entries (256 per
+# 16 x 16 block holding a nonzero) per nonzero.
+BSR_FILL_MAX = 2.0
+
+
+class BsrPlan:
+    """The tensor-core BSR path as an SpMM plan: the CSR matrix is converted
+    once (``bsr.csr_to_bsr16``, cached on the plan for that matrix) and each
+    call runs ``fsb_bsr_spmm_tc``.  Runs only half-precision values with a
+    same-typed B, a float32 C with a multiple of 8 columns and float32
+    accumulation; ValueError otherwise, or when the 16 x 16 blocks would
+    store more than BSR_FILL_MAX entries per nonzero."""
+
+    algo = ALGO_BSR
+    flags = 0
+    n_tile = 0
+    items_per_unit = 0
+    lanes = 0
+    grid_blocks = 0
+
+    def __init__(self):
+        self.comp_threshold = 0
+        self._form = None  # (matrix key, PreparedBsr)
+
+    def key(self):
+        return (ALGO_BSR,)
+
+    def describe(self):
+        return {"kind": "bsr16_tcgen05"}
+
+    def copy(self):
+        return BsrPlan()
+
+    def in_kernel_finish(self):
+        return True
+
+    def ensure_coords(self, row_ptr, n_rows, nnz):
+        return
+
+    def ensure_runs(self, row_ptr, n_rows, n_dense):
+        return
+
+    @staticmethod
+    def supported(values, B, C, acc_mode, row_map=None):
+        return (values.dtype in (torch.bfloat16, torch.float16) and B.dtype == values.dtype and
+                C.dtype == torch.float32 and C.is_contiguous() and B.shape[1] % 8 == 0 and row_map is None and
+                int(acc_mode) == nat.ACC_NATIVE)
+
+    def prepared(self, values, col_idx, row_ptr, n_rows, n_cols):
+        from . import bsr
+
+        key = (values.data_ptr(), col_idx.data_ptr(), row_ptr.data_ptr(), int(values.numel()), int(n_rows),
+               int(n_cols))
+        if self._form is None or self._form[0] != key:
+            blocks = bsr.block_count(col_idx, row_ptr, (n_rows, n_cols))
+            if blocks * bsr.BLOCK * bsr.BLOCK > BSR_FILL_MAX * max(int(values.numel()), 1):
+                raise ValueError(f"BSR fill-in too high: {blocks} blocks for {int(values.numel())} nonzeros")
+            vals, bcol, bptr = bsr.csr_to_bsr16(values, col_idx, row_ptr, (n_rows, n_cols))
+            self._form = (key, bsr.prepare_spmm_bsr(vals, bcol, bptr, (n_rows, n_cols)))
+        return self._form[1]
+
+    def run(self, values, col_idx, row_ptr, n_rows, n_cols, B, C, acc_mode, row_map=None):
+        from . import bsr
+
+        if not self.supported(values, B, C, acc_mode, row_map):
+            raise ValueError("the BSR plan needs half-precision values and B, a float32 C with a multiple of 8 "
+                             "columns and float32 accumulation")
+        bsr.flagsparse_spmm_bsr(B=B, prepared=self.prepared(values, col_idx, row_ptr, n_rows, n_cols), out=C)
+        return C
 
 
 # Split rows finish inside the SEQ kernel while at most this many units hold
@@ -472,6 +545,8 @@ def g4_supported(values, B, C, acc_mode, n_cols):
 
 def run_spmm(values, col_idx, row_ptr, n_rows, n_cols, B, C, acc_mode, plan, row_map=None):
     """C = A B through fsb_spmm_csr (B, C row-major with unit column stride)."""
+    if isinstance(plan, BsrPlan):
+        return plan.run(values, col_idx, row_ptr, n_rows, n_cols, B, C, acc_mode, row_map)
     if plan.algo == nat.ALGO_GATHER and not gather_supported(B, C, plan.n_tile):
         if not plan.fallback_ok:
             raise ValueError("the TMA gather plan needs 16-byte aligned B and C rows")

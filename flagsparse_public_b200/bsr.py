@@ -21,6 +21,20 @@ BLOCK = 16
 BSR_VALUE_DTYPES = (torch.bfloat16, torch.float16)
 
 
+def block_count(indices, indptr, shape):
+    """Number of 16 x 16 blocks holding at least one nonzero (the blocks
+    csr_to_bsr16 stores), computed on the device without building them."""
+    n_rows, n_cols = int(shape[0]), int(shape[1])
+    nnz = int(indices.numel())
+    if nnz == 0:
+        return 0
+    nbc = (n_cols + BLOCK - 1) // BLOCK
+    lens = (indptr[1:] - indptr[:-1]).to(torch.int64)
+    row = torch.repeat_interleave(torch.arange(n_rows, device=indices.device), lens, output_size=nnz)
+    key = (row // BLOCK) * nbc + indices.to(torch.int64) // BLOCK
+    return int(torch.unique(key).numel())
+
+
 def csr_to_bsr16(data, indices, indptr, shape, dtype=None):
     """(block_values [n_blocks, 16, 16], block_col int32, block_row_ptr int64)
     of the 16 x 16 blocks holding the CSR matrix's nonzeros (sorted by block

@@ -27,10 +27,10 @@ constexpr int kMlpMaxOut = 32;
 template <class I, class P>
 __global__ void __launch_bounds__(256) k_csr_features(const P* __restrict__ ptr, const I* __restrict__ col,
                                                       int64_t n_rows, int64_t n_cols, double* __restrict__ out) {
-    __shared__ double s_sum[8], s_sq[8], s_band[8], s_empty[8];
+    __shared__ double s_sum[8], s_sq[8], s_band[8], s_empty[8], s_aligned[8];
     __shared__ unsigned long long s_max[8];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    double sum = 0, sq = 0, band = 0, empty = 0;
+    double sum = 0, sq = 0, band = 0, empty = 0, aligned = 0;
     unsigned long long mx = 0;
     const double scale = n_rows > 0 ? (double)n_cols / (double)n_rows : 0.0;
     const double inv_cols = n_cols > 0 ? 1.0 / (double)n_cols : 0.0;
@@ -44,25 +44,36 @@ __global__ void __launch_bounds__(256) k_csr_features(const P* __restrict__ ptr,
             if ((unsigned long long)(e - s) > mx) mx = (unsigned long long)(e - s);
         }
         const double diag = (double)r * scale;
-        for (int64_t k = s + lane; k < e; k += 32) band += fabs((double)idx(col[k]) - diag) * inv_cols;
+        for (int64_t k = s + lane; k < e; k += 32) {
+            const int64_t c = idx(col[k]);
+            band += fabs((double)c - diag) * inv_cols;
+            // in a row of aligned dense 16-column blocks, column and position
+            // in the row agree modulo 16
+            aligned += ((c & 15) == ((k - s) & 15)) ? 1.0 : 0.0;
+        }
     }
-    for (int o = 16; o > 0; o >>= 1) band += __shfl_xor_sync(0xffffffffu, band, o);
+    for (int o = 16; o > 0; o >>= 1) {
+        band += __shfl_xor_sync(0xffffffffu, band, o);
+        aligned += __shfl_xor_sync(0xffffffffu, aligned, o);
+    }
     if (lane == 0) {
         s_sum[warp] = sum;
         s_sq[warp] = sq;
         s_band[warp] = band;
         s_empty[warp] = empty;
+        s_aligned[warp] = aligned;
         s_max[warp] = mx;
     }
     __syncthreads();
     if (threadIdx.x == 0) {
-        double a = 0, b = 0, c = 0, d = 0;
+        double a = 0, b = 0, c = 0, d = 0, al = 0;
         unsigned long long m = 0;
         for (int w = 0; w < 8; ++w) {
             a += s_sum[w];
             b += s_sq[w];
             c += s_band[w];
             d += s_empty[w];
+            al += s_aligned[w];
             m = s_max[w] > m ? s_max[w] : m;
         }
         atomicAdd(out + 0, a);
@@ -70,6 +81,7 @@ __global__ void __launch_bounds__(256) k_csr_features(const P* __restrict__ ptr,
         atomicMax(reinterpret_cast<unsigned long long*>(out + 2), m);  // integer held in the slot's bits
         atomicAdd(out + 3, d);
         atomicAdd(out + 4, c);
+        atomicAdd(out + 5, al);
     }
 }
 

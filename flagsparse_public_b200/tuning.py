@@ -78,7 +78,12 @@ SPMM_CANDIDATES = (
     ("seq1024", _seq(1024)),
     ("seq256_t32", _seq(256, 32)),
     ("seq1024_t32", _seq(1024, 32)),
+    ("bsr16_tc", _plan.BsrPlan),  # half-precision values only; 16 x 16 blocks on the tensor cores
 )
+BSR_CANDIDATE = len(SPMM_CANDIDATES) - 1
+# The BSR candidate is offered to the network only for matrices whose
+# nonzeros mostly sit as in aligned dense 16-column blocks (feature 11).
+BSR_ALIGNED_MIN = 0.5
 CANDIDATE_NAMES = tuple(n for n, _ in SPMM_CANDIDATES)
 
 
@@ -87,7 +92,7 @@ def raw_features(indices, indptr, n_rows, n_cols, n_dense, value_bytes=4):
     """Feature vector (float64, N_FEATURES) of a CSR matrix and dense width,
     the structure sums computed on the device by fsb_csr_features."""
     n_rows, n_cols = int(n_rows), int(n_cols)
-    out = torch.zeros(5, dtype=torch.float64, device=indptr.device)
+    out = torch.zeros(6, dtype=torch.float64, device=indptr.device)
     if n_rows > 0:
         lib = nat.library()
         rc = lib.fsb_csr_features(nat.ptr(indptr), nat.dtype_code(indptr.dtype), nat.ptr(indices),
@@ -98,10 +103,11 @@ def raw_features(indices, indptr, n_rows, n_cols, n_dense, value_bytes=4):
     s = host.numpy()
     max_len = int(host.view(torch.int64)[2].item())
     return features_from_sums(n_rows, n_cols, float(s[0]), float(s[1]), max_len, float(s[3]), float(s[4]),
-                              n_dense, value_bytes)
+                              n_dense, value_bytes, float(s[5]))
 
 
-def features_from_sums(n_rows, n_cols, sum_len, sum_sq, max_len, empty, band_sum, n_dense, value_bytes=4):
+def features_from_sums(n_rows, n_cols, sum_len, sum_sq, max_len, empty, band_sum, n_dense, value_bytes=4,
+                       aligned=0.0):
     nnz = sum_len
     mean = nnz / max(n_rows, 1)
     var = max(sum_sq / max(n_rows, 1) - mean * mean, 0.0)
@@ -119,7 +125,7 @@ def features_from_sums(n_rows, n_cols, sum_len, sum_sq, max_len, empty, band_sum
     f[8] = band
     f[9] = empty / max(n_rows, 1)
     f[10] = math.log2(n_dense)
-    f[11] = 1.0 if n_dense % 4 == 0 else 0.0
+    f[11] = aligned / max(nnz, 1.0)  # share of nonzeros placed as in aligned dense 16-column blocks
     f[12] = math.log2(n_dense * value_bytes * n_cols + 1)  # dense operand bytes
     f[13] = math.log2(nnz * n_dense + 1)  # multiply-adds
     f[14] = value_bytes / 8.0
@@ -296,9 +302,12 @@ class LearnedSelector:
         X = torch.from_numpy(np.atleast_2d(self.standardize(features))).to(self.mlp.params.device)
         return self.mlp.forward(X).cpu().numpy()
 
-    def choose(self, f):
-        """(candidate index, confident?) for one raw feature vector."""
+    def choose(self, f, feasible=None):
+        """(candidate index, confident?) for one raw feature vector; only
+        candidates marked feasible (all by default) can be picked."""
         pred = self.predict(f)[0]
+        if feasible is not None:
+            pred = np.where(np.asarray(feasible, dtype=bool), pred, np.inf)
         order = np.argsort(pred)
         z = (np.asarray(f) - self.mu) / self.sigma
         in_range = bool(np.all(np.abs(z) <= self.z_limit))
@@ -308,7 +317,19 @@ class LearnedSelector:
     def select(self, data, indices, indptr, n_rows, n_cols, B, C, acc_mode):
         """Plan for these operands: the network's pick, or the autotuner's."""
         f = raw_features(indices, indptr, n_rows, n_cols, B.shape[1], data.element_size())
-        k, confident = self.choose(f)
+        feasible = np.ones(len(SPMM_CANDIDATES), dtype=bool)
+        feasible[BSR_CANDIDATE] = f[11] >= BSR_ALIGNED_MIN and _plan.BsrPlan.supported(data, B, C, acc_mode)
+        k, confident = self.choose(f, feasible)
+        if confident and k == BSR_CANDIDATE:
+            plan = _plan.BsrPlan()
+            try:
+                plan.prepared(data, indices, indptr, n_rows, n_cols)  # fill-in check, conversion cached
+            except ValueError:
+                feasible[BSR_CANDIDATE] = False
+                k, confident = self.choose(f, feasible)
+            else:
+                self.last = ("learned", CANDIDATE_NAMES[k])
+                return plan
         if confident:
             self.last = ("learned", CANDIDATE_NAMES[k])
             return SPMM_CANDIDATES[k][1]()
@@ -322,10 +343,12 @@ FAMILIES = ("poisson", "zipf", "banded", "block16", "rect2")
 
 
 def corpus_specs(n_train=2000, n_test=400, seed=0, min_rows=10_000, max_rows=2_000_000, min_mean=2.0,
-                 max_mean=128.0, nnz_cap=1 << 24):
+                 max_mean=128.0, nnz_cap=1 << 24, n_large=0):
     """Seeded matrix specs (family, rows, mean, seed, split), families in
     rotation; rows and mean log-uniform; rows shrunk where rows x mean would
-    exceed nnz_cap."""
+    exceed nnz_cap.  ``n_large`` more held-out specs (split "large") draw
+    rows and mean from the same ranges until rows x mean exceeds nnz_cap:
+    the sizes above the cap, up to 2e6 rows x 128 nonzeros."""
     rng = np.random.default_rng(seed)
     specs = []
     for i in range(n_train + n_test):
@@ -336,7 +359,23 @@ def corpus_specs(n_train=2000, n_test=400, seed=0, min_rows=10_000, max_rows=2_0
             rows = max(min_rows, int(nnz_cap / mean))
         specs.append({"family": fam, "rows": rows, "mean": mean, "seed": int(rng.integers(1 << 30)),
                       "split": "train" if i < n_train else "test"})
+    big = np.random.default_rng(seed + 1)
+    for i in range(n_large):
+        while True:
+            rows = int(round(math.exp(big.uniform(math.log(min_rows), math.log(max_rows)))))
+            mean = float(math.exp(big.uniform(math.log(min_mean), math.log(max_mean))))
+            if rows * mean > nnz_cap:
+                break
+        specs.append({"family": FAMILIES[i % len(FAMILIES)], "rows": rows, "mean": mean,
+                      "seed": int(big.integers(1 << 30)), "split": "large"})
     return specs
+
+
+def value_dtype(spec):
+    """Value (and dense operand) type of a corpus matrix: the block-sparse
+    family is bfloat16 (the tensor-core BSR candidate's type), the others
+    float32."""
+    return torch.bfloat16 if spec["family"] == "block16" else torch.float32
 
 
 def build_matrix(spec, device="cuda", dtype=torch.float32):
@@ -361,16 +400,18 @@ def build_matrix(spec, device="cuda", dtype=torch.float32):
 
 
 def collect(specs, device="cuda", n_values=N_VALUES, log=None):
-    """Features and per-candidate times (ms, float32 native accumulation) for
-    every (matrix, N); returns dict of numpy arrays."""
+    """Features and per-candidate times (ms, float32 accumulation and result;
+    values and B in value_dtype(spec)) for every (matrix, N); returns dict of
+    numpy arrays."""
     feats, times, mat, nval = [], [], [], []
     t_start = time.time()
     for i, spec in enumerate(specs):
-        data, indices, indptr, (n_rows, n_cols) = build_matrix(spec, device)
+        vdt = value_dtype(spec)
+        data, indices, indptr, (n_rows, n_cols) = build_matrix(spec, device, dtype=vdt)
         for n_dense in n_values:
-            B = synthetic.dense_operand(n_cols, n_dense, seed=spec["seed"] + n_dense, device=device)
+            B = synthetic.dense_operand(n_cols, n_dense, seed=spec["seed"] + n_dense, dtype=vdt, device=device)
             C = torch.empty((n_rows, n_dense), dtype=torch.float32, device=device)
-            feats.append(raw_features(indices, indptr, n_rows, n_cols, n_dense, 4))
+            feats.append(raw_features(indices, indptr, n_rows, n_cols, n_dense, data.element_size()))
             times.append(time_candidates(data, indices, indptr, n_rows, n_cols, B, C, nat.ACC_NATIVE))
             mat.append(i)
             nval.append(n_dense)
@@ -380,6 +421,17 @@ def collect(specs, device="cuda", n_values=N_VALUES, log=None):
             log(f"{i + 1}/{len(specs)} matrices, {time.time() - t_start:.0f} s")
     return {"features": np.asarray(feats, dtype=np.float64), "times": np.asarray(times, dtype=np.float64),
             "matrix": np.asarray(mat, dtype=np.int64), "n_dense": np.asarray(nval, dtype=np.int64)}
+
+
+def selectable(features, times):
+    """0/1 per (sample, candidate): the candidate ran (finite time) and the
+    selector may offer it (the BSR candidate only for half-precision values
+    placed mostly as aligned 16-column blocks), as LearnedSelector.select
+    decides from the same features."""
+    F = np.atleast_2d(np.asarray(features, dtype=np.float64))
+    ok = np.isfinite(np.asarray(times, dtype=np.float64))
+    ok[:, BSR_CANDIDATE] &= (F[:, 11] >= BSR_ALIGNED_MIN) & (F[:, 14] <= 0.25)
+    return ok
 
 
 def heuristic_choice(features):
@@ -417,6 +469,7 @@ def main(argv=None):
     ap.add_argument("--train", type=int, default=2000)
     ap.add_argument("--test", type=int, default=400)
     ap.add_argument("--nnz-cap", type=int, default=1 << 24)
+    ap.add_argument("--large", type=int, default=0, help="held-out matrices above the nnz cap")
     ap.add_argument("--steps", type=int, default=4000)
     ap.add_argument("--dataset", default=None, help="reuse a timing dataset (.npz) instead of timing")
     ap.add_argument("--save-dataset", default=None)
@@ -426,14 +479,17 @@ def main(argv=None):
     dev = torch.device("cuda")
     if args.dataset:
         z = np.load(args.dataset, allow_pickle=False)
-        data = {k: z[k] for k in ("features", "times", "matrix", "n_dense", "split")}
+        data = {k: z[k] for k in ("features", "times", "matrix", "n_dense", "split", "kind")}
     else:
-        specs = corpus_specs(args.train, args.test, nnz_cap=args.nnz_cap)
+        specs = corpus_specs(args.train, args.test, nnz_cap=args.nnz_cap, n_large=args.large)
         data = collect(specs, dev, log=lambda s: print(s, flush=True))
-        data["split"] = np.asarray([specs[m]["split"] == "train" for m in data["matrix"]], dtype=np.bool_)
+        kinds = ("train", "test", "large")
+        data["kind"] = np.asarray([kinds.index(specs[m]["split"]) for m in data["matrix"]], dtype=np.int8)
+        data["split"] = data["kind"] == 0
         if args.save_dataset:
             np.savez_compressed(args.save_dataset, **data, names=np.asarray(CANDIDATE_NAMES))
     F, Tm, is_train = data["features"], data["times"], data["split"].astype(bool)
+    kind = data["kind"]
     mu, sigma = fit_standardisation(F[is_train])
     T, M = targets_from_times(Tm)
     X = ((F - mu) / sigma).astype(np.float32)
@@ -441,25 +497,30 @@ def main(argv=None):
     t0 = time.time()
     mlp, losses = train_mlp(to(X[is_train]), to(T[is_train]), to(M[is_train]), steps=args.steps)
     train_s = time.time() - t0
-    pred = mlp.forward(to(X[~is_train])).cpu().numpy()
-    learned = np.argmin(np.where(M[~is_train] > 0, pred, np.inf), axis=1)
-    heur = np.asarray([heuristic_choice(f) for f in F[~is_train]])
-    r_learned = regret(Tm[~is_train], learned)
-    r_heur = regret(Tm[~is_train], heur)
-    total = lambda c: float(np.sum(Tm[~is_train][np.arange(len(c)), c]))  # noqa: E731
-    best_total = float(np.sum(np.where(np.isfinite(Tm[~is_train]), Tm[~is_train], np.inf).min(axis=1)))
-    report = {
-        "samples_train": int(is_train.sum()), "samples_test": int((~is_train).sum()),
-        "train_seconds": train_s, "final_loss": float(losses[-1]),
-        "test_total_ms": {"autotune": best_total, "learned": total(learned), "heuristic": total(heur)},
-        "learned_over_autotune": total(learned) / best_total,
-        "heuristic_over_autotune": total(heur) / best_total,
-        "regret_learned": {"mean": float(r_learned.mean()), "median": float(np.median(r_learned)),
-                           "p90": float(np.percentile(r_learned, 90)), "max": float(r_learned.max())},
-        "regret_heuristic": {"mean": float(r_heur.mean()), "median": float(np.median(r_heur)),
-                             "p90": float(np.percentile(r_heur, 90)), "max": float(r_heur.max())},
-        "exact_pick_rate": float(np.mean(r_learned <= 1.0 + 1e-9)),
-    }
+    report = {"samples_train": int(is_train.sum()), "train_seconds": train_s, "final_loss": float(losses[-1])}
+    for name, sel in (("test", kind == 1), ("large", kind == 2)):
+        if not sel.any():
+            continue
+        pred = mlp.forward(to(X[sel])).cpu().numpy()
+        learned = np.argmin(np.where(selectable(F[sel], Tm[sel]), pred, np.inf), axis=1)
+        heur = np.asarray([heuristic_choice(f) for f in F[sel]])
+        r_learned = regret(Tm[sel], learned)
+        r_heur = regret(Tm[sel], heur)
+        total = lambda c: float(np.sum(Tm[sel][np.arange(len(c)), c]))  # noqa: E731
+        best_total = float(np.sum(np.where(np.isfinite(Tm[sel]), Tm[sel], np.inf).min(axis=1)))
+        report[name] = {
+            "samples": int(sel.sum()),
+            "total_ms": {"autotune": best_total, "learned": total(learned), "heuristic": total(heur)},
+            "learned_over_autotune": total(learned) / best_total,
+            "heuristic_over_autotune": total(heur) / best_total,
+            "regret_learned": {"mean": float(r_learned.mean()), "median": float(np.median(r_learned)),
+                               "p90": float(np.percentile(r_learned, 90)), "max": float(r_learned.max())},
+            "regret_heuristic": {"mean": float(r_heur.mean()), "median": float(np.median(r_heur)),
+                                 "p90": float(np.percentile(r_heur, 90)), "max": float(r_heur.max())},
+            "exact_pick_rate": float(np.mean(r_learned <= 1.0 + 1e-9)),
+            "bsr_best": int(np.sum(np.argmin(np.where(np.isfinite(Tm[sel]), Tm[sel], np.inf), axis=1) == BSR_CANDIDATE)),
+            "bsr_picked": int(np.sum(learned == BSR_CANDIDATE)),
+        }
     print(json.dumps(report, indent=1), flush=True)
     save_weights(args.weights, mlp, mu, sigma, F[is_train].min(0), F[is_train].max(0),
                  {"report": report, "steps": args.steps})

@@ -484,12 +484,14 @@ void  fsb_mtx_close(void* handle);
  * (spmm_csr.py:395-414, spmm_csr_opt_alg2.py:175-304).  These entry points
  * are the device side of the learned selector that replaces them.         */
 
-/* Structure features of a CSR matrix (five doubles, written on stream):
- * out[0] = sum of row lengths, out[1] = sum of squared row lengths,
- * out[2] = longest row (an unsigned 64-bit integer held in the slot's bits),
- * out[3] = empty rows, out[4] = sum over nonzeros of
- * |col - r * n_cols / n_rows| / n_cols.  Sums of doubles are accumulated
- * with atomics (last-bit order dependence).                               */
+/* Structure features of a CSR matrix (six doubles, zeroed by the caller,
+ * accumulated on stream): out[0] = sum of row lengths, out[1] = sum of
+ * squared row lengths, out[2] = longest row (an unsigned 64-bit integer
+ * held in the slot's bits), out[3] = empty rows, out[4] = sum over nonzeros
+ * of |col - r * n_cols / n_rows| / n_cols, out[5] = nonzeros whose column
+ * and position in the row agree modulo 16 (all of them when the rows are
+ * aligned dense 16-column blocks).  Sums of doubles are accumulated with
+ * atomics (last-bit order dependence).                                    */
 int fsb_csr_features(const void* row_ptr, int ptr_dtype, const void* col_idx,
                      int index_dtype, int64_t n_rows, int64_t n_cols,
                      double* out, void* stream);

@@ -20,8 +20,11 @@ def _host_sums(indices, indptr, n_rows, n_cols):
     lens = (indptr[1:] - indptr[:-1]).to(torch.float64)
     row = torch.repeat_interleave(torch.arange(n_rows, dtype=torch.float64), (indptr[1:] - indptr[:-1]))
     band = ((indices.to(torch.float64) - row * (n_cols / n_rows)).abs() / n_cols).sum()
+    starts = torch.repeat_interleave(indptr[:-1].long(), (indptr[1:] - indptr[:-1]))
+    pos = torch.arange(indices.numel()) - starts
+    aligned = int(((indices.long() & 15) == (pos & 15)).sum())
     return lens.sum().item(), (lens * lens).sum().item(), int(lens.max().item()), int((lens == 0).sum().item()), \
-        band.item()
+        band.item(), aligned
 
 
 @pytest.mark.parametrize("idx_dtype,ptr_dtype", [(torch.int32, torch.int64), (torch.int64, torch.int32)])
@@ -29,16 +32,17 @@ def test_features_kernel_matches_host_sums(idx_dtype, ptr_dtype):
     data, indices, indptr, (n_rows, n_cols) = synthetic.zipf_powerlaw(5000, 3000, mean=7.0, cap=900, seed=4,
                                                                        device="cpu")
     indices, indptr = indices.to(idx_dtype), indptr.to(ptr_dtype)
-    out = torch.zeros(5, dtype=torch.float64, device=DEV)
+    out = torch.zeros(6, dtype=torch.float64, device=DEV)
     ptr_d, idx_d = indptr.to(DEV), indices.to(DEV)  # kept alive across the launch
     rc = nat.library().fsb_csr_features(nat.ptr(ptr_d), nat.dtype_code(ptr_dtype), nat.ptr(idx_d),
                                         nat.dtype_code(idx_dtype), n_rows, n_cols, nat.ptr(out),
                                         nat.stream_handle(torch.device(DEV)))
     torch.cuda.synchronize()
     nat.check(rc, "fsb_csr_features")
-    s, sq, mx, empty, band = _host_sums(indices.long(), indptr.long(), n_rows, n_cols)
+    s, sq, mx, empty, band, aligned = _host_sums(indices.long(), indptr.long(), n_rows, n_cols)
     got = out.cpu()
     assert got[0].item() == s and got[1].item() == sq and got[3].item() == empty
+    assert got[5].item() == aligned
     assert int(got.view(torch.int64)[2].item()) == mx
     assert got[4].item() == pytest.approx(band, rel=1e-12)
 
@@ -157,3 +161,29 @@ def test_learned_selector_runs_its_pick():
         _plan.run_spmm(data, indices, indptr, n_rows, n_cols, B, C, nat.ACC_NATIVE, plan)
         ref = torch.sparse_csr_tensor(indptr, indices.long(), data.double(), size=(n_rows, n_cols)) @ B.double()
         assert float((C.double() - ref).abs().max() / ref.abs().max()) < 1e-5
+
+
+def test_bsr_candidate_runs_through_run_spmm():
+    """The selector's tensor-core BSR candidate (a BsrPlan) through the plan
+    interface: bfloat16 block-sparse matrix against FP64 of the same inputs;
+    refused (ValueError) for float32 values and for scattered matrices whose
+    16 x 16 blocks would be mostly zeros."""
+    data, indices, indptr, (n_rows, n_cols) = synthetic.block_sparse(300, 3, seed=5, dtype=torch.bfloat16,
+                                                                     device=DEV)
+    B = synthetic.dense_operand(n_cols, 32, seed=6, dtype=torch.bfloat16, device=DEV)
+    C = torch.full((n_rows, 32), float("nan"), device=DEV)
+    plan = tuning.SPMM_CANDIDATES[tuning.BSR_CANDIDATE][1]()
+    _plan.run_spmm(data, indices, indptr, n_rows, n_cols, B, C, nat.ACC_NATIVE, plan)
+    A = torch.sparse_csr_tensor(indptr.cpu(), indices.long().cpu(), data.double().cpu(), size=(n_rows, n_cols))
+    ref = A @ B.double().cpu()
+    mag = A.abs() @ B.double().abs().cpu()
+    assert float(((C.cpu().double() - ref).abs() / mag.clamp(min=1e-300)).max()) <= 1e-5
+    f = tuning.raw_features(indices, indptr, n_rows, n_cols, 32, 2)
+    assert f[11] == 1.0  # every nonzero sits as in an aligned dense 16-column block
+    with pytest.raises(ValueError):
+        _plan.run_spmm(data.float(), indices, indptr, n_rows, n_cols, B.float(), C, nat.ACC_NATIVE,
+                       _plan.BsrPlan())
+    sd, si, sp, (sr, sc) = synthetic.poisson_uniform(4000, 4000, mean=8.0, seed=7, dtype=torch.bfloat16, device=DEV)
+    Bs = synthetic.dense_operand(sc, 32, seed=8, dtype=torch.bfloat16, device=DEV)
+    with pytest.raises(ValueError, match="fill-in"):
+        _plan.run_spmm(sd, si, sp, sr, sc, Bs, torch.empty((sr, 32), device=DEV), nat.ACC_NATIVE, _plan.BsrPlan())
