@@ -109,6 +109,14 @@ __device__ __forceinline__ void st_stream1(T* p, T v) {
 // Indices: 64-bit arithmetic everywhere, whatever the stored width.
 template <class I> __device__ __forceinline__ int64_t idx(I v) { return (int64_t)v; }
 
+// bfloat16 is the upper half of a float32: widening is a 16-bit shift on the
+// integer pipe (exact)
+__device__ __forceinline__ float widen_bf16(__nv_bfloat16 v) {
+    unsigned short u;
+    memcpy(&u, &v, 2);
+    return __uint_as_float((unsigned)u << 16);
+}
+
 // ------------------------------------------------------ accumulator ops ----
 // Acc<V, A>: how a product of two V values enters an A accumulator.
 template <class V, class A> struct Acc;
@@ -125,7 +133,7 @@ FSB_REAL_ACC(float, float, FSB_ID)
 FSB_REAL_ACC(float, double, FSB_ID)
 FSB_REAL_ACC(double, double, FSB_ID)
 FSB_REAL_ACC(__half, float, __half2float)
-FSB_REAL_ACC(__nv_bfloat16, float, __bfloat162float)
+FSB_REAL_ACC(__nv_bfloat16, float, widen_bf16)
 #undef FSB_REAL_ACC
 
 template <> struct Acc<c64_t, c64_t> {
@@ -175,7 +183,7 @@ template <> struct Acc<c128_t, c128_t> {
 
 __device__ __forceinline__ float to_f32(float v) { return v; }
 __device__ __forceinline__ float to_f32(__half v) { return __half2float(v); }
-__device__ __forceinline__ float to_f32(__nv_bfloat16 v) { return __bfloat162float(v); }
+__device__ __forceinline__ float to_f32(__nv_bfloat16 v) { return widen_bf16(v); }
 
 // TwoSum (Knuth): s + p = t + e exactly.
 __device__ __forceinline__ comp_t comp_add_value(comp_t acc, float p, float p_err) {

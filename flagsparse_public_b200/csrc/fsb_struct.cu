@@ -446,6 +446,34 @@ __device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t
                  : "memory");
 }
 
+// Float32 pairs in one 64-bit register (low word: the first element).
+__device__ __forceinline__ uint64_t lt_fma2(uint64_t a, uint64_t b, uint64_t c) {
+    uint64_t d;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(d) : "l"(a), "l"(b), "l"(c));
+    return d;
+}
+__device__ __forceinline__ uint64_t lt_splat(float a) {
+    const uint64_t u = __float_as_uint(a);
+    return u | (u << 32);
+}
+// A 16-bit value held in the low bits of a record, as float32.
+template <class V> __device__ __forceinline__ float lt_value(uint32_t bits);
+template <> __device__ __forceinline__ float lt_value<__nv_bfloat16>(uint32_t bits) {
+    return __uint_as_float(bits << 16);
+}
+template <> __device__ __forceinline__ float lt_value<__half>(uint32_t bits) {
+    return __half2float(__ushort_as_half((unsigned short)bits));
+}
+// Two 16-bit values of a 32-bit word (the first in the low half) as a float32 pair.
+template <class V> __device__ __forceinline__ uint64_t lt_widen2(uint32_t w);
+template <> __device__ __forceinline__ uint64_t lt_widen2<__nv_bfloat16>(uint32_t w) {
+    return (uint64_t)(w << 16) | ((uint64_t)(w & 0xffff0000u) << 32);
+}
+template <> __device__ __forceinline__ uint64_t lt_widen2<__half>(uint32_t w) {
+    const float2 f = __half22float2(*reinterpret_cast<const __half2*>(&w));
+    return (uint64_t)__float_as_uint(f.x) | ((uint64_t)__float_as_uint(f.y) << 32);
+}
+
 template <class V, int N>
 __global__ void __launch_bounds__(kLtThreads, 1)
 k_struct_spmm_ltile(const uint32_t* __restrict__ rec, const int64_t* __restrict__ seg_start,
@@ -511,41 +539,35 @@ k_struct_spmm_ltile(const uint32_t* __restrict__ rec, const int64_t* __restrict_
         for (int i = 0; i < RPS; ++i) {
             const int rig = rig0 + i;
             const int lo = rs[rig], hi = rs[rig + 1];
-            float blk[VW];
+            // the row's products of this block, summed plainly in float32
+            // pairs: blk[h] holds columns 2h, 2h + 1 of the lane's slice
+            uint64_t blk[VW / 2];
 #pragma unroll
-            for (int w = 0; w < VW; ++w) blk[w] = 0.f;
-            // B row slices as single 16-byte shared loads (the slice is
-            // 16-byte aligned: row * N * 2 + lig * 16 bytes)
-            auto slice = [&](uint32_t rr) -> vec_t<V, VW> {
+            for (int h = 0; h < VW / 2; ++h) blk[h] = 0;
+            // one record: the B row slice as a single 16-byte shared load (the
+            // slice is 16-byte aligned: row * N * 2 + lig * 16 bytes), widened
+            // to float32 pairs, times the value, added by paired FMAs
+            auto step = [&](uint32_t rr) {
                 const uint4 q4 = *reinterpret_cast<const uint4*>(Bs + (rr >> 16) * N + lig * VW);
-                vec_t<V, VW> out;
-                memcpy(&out, &q4, 16);
-                return out;
-            };
-            auto value = [&](uint32_t rr) -> float {
-                V a;
-                const unsigned short u = (unsigned short)(rr & 0xffffu);
-                memcpy(&a, &u, 2);
-                return to_f32(a);
+                const uint64_t a2 = lt_splat(lt_value<V>(rr & 0xffffu));
+                blk[0] = lt_fma2(a2, lt_widen2<V>(q4.x), blk[0]);
+                blk[1] = lt_fma2(a2, lt_widen2<V>(q4.y), blk[1]);
+                blk[2] = lt_fma2(a2, lt_widen2<V>(q4.z), blk[2]);
+                blk[3] = lt_fma2(a2, lt_widen2<V>(q4.w), blk[3]);
             };
             int k = lo;
             for (; k + 1 < hi; k += 2) {  // two independent records in flight
                 const uint32_t r0 = rc[k], r1 = rc[k + 1];
-                const vec_t<V, VW> b0 = slice(r0), b1 = slice(r1);
-                const float fa0 = value(r0), fa1 = value(r1);
-#pragma unroll
-                for (int w = 0; w < VW; ++w) blk[w] = fmaf(fa1, to_f32(b1.v[w]), fmaf(fa0, to_f32(b0.v[w]), blk[w]));
+                step(r0);
+                step(r1);
             }
-            if (k < hi) {
-                const uint32_t r0 = rc[k];
-                const vec_t<V, VW> b0 = slice(r0);
-                const float fa0 = value(r0);
-#pragma unroll
-                for (int w = 0; w < VW; ++w) blk[w] = fmaf(fa0, to_f32(b0.v[w]), blk[w]);
-            }
+            if (k < hi) step(rc[k]);
             if (hi > lo) {
 #pragma unroll
-                for (int w = 0; w < VW; ++w) acc[i][w] = comp_add_value(acc[i][w], blk[w], 0.f);
+                for (int h = 0; h < VW / 2; ++h) {
+                    acc[i][2 * h] = comp_add_value(acc[i][2 * h], __uint_as_float((uint32_t)blk[h]), 0.f);
+                    acc[i][2 * h + 1] = comp_add_value(acc[i][2 * h + 1], __uint_as_float((uint32_t)(blk[h] >> 32)), 0.f);
+                }
             }
         }
         __syncthreads();  // stage st is free for block j + 2
