@@ -76,3 +76,22 @@ def test_precision_api_validation(banded):
     out = torch.empty(shape[0], device=DEV)
     y, ms = fs.flagsparse_spmv_csr_mixed(x=x.bfloat16(), prepared=p, out=out, return_time=True)
     assert y is out and isinstance(ms, float)
+
+
+def test_precision_spmm_of_a_block_matrix_runs_on_the_tensor_core_bsr_plan():
+    """A bfloat16 matrix of dense 16 x 16 blocks through the public precision
+    API: the learned selector picks the tensor-core BSR candidate, and the
+    result is within float32 accumulation of FP64 of the same inputs."""
+    from flagsparse_public_b200 import _plan, synthetic, tuning
+
+    if _plan.learned_selector(torch.device(DEV)) is None:
+        pytest.skip("no selector weights installed")
+    data, indices, indptr, shape = synthetic.block_sparse(8192, 6, seed=11, dtype=torch.bfloat16, device=DEV)
+    B = synthetic.dense_operand(shape[1], 128, seed=12, dtype=torch.bfloat16, device=DEV)
+    prepared = fs.prepare_csr_mixed(data, indices, indptr, shape, layout="csr")
+    C, err = fs.flagsparse_spmm_csr_mixed(B=B, prepared=prepared, return_error=True)
+    plan = prepared._plans[("spmm", 128)]
+    assert isinstance(plan, _plan.BsrPlan), plan.describe()
+    assert err <= 1e-5
+    f = tuning.raw_features(indices, indptr, shape[0], shape[1], 128, 2)
+    assert f[11] == 1.0
