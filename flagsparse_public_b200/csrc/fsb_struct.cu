@@ -426,15 +426,16 @@ __global__ void k_struct_spmm_fold(const comp_t* __restrict__ partial, const int
 // block) segment, the group's nonzeros in that block ordered by row, each as
 // one 32-bit record (16-bit value bits | column inside the block << 16),
 // padded to 16 bytes, with the segment's per-row record starts (kLtRsEntries
-// 16-bit entries).  One CTA of 1024 threads per (group, column range): block
-// by block, one thread brings the B block (contiguous B rows), the row starts
-// and the records into a shared-memory stage with bulk copies (completion on
-// the stage's mbarrier, bounded waits) while the CTA multiplies the previous
-// block entirely out of shared memory: LPN = N / 8 lanes per row, 8 columns
-// (16 bytes) per lane, each row's products of a block summed plainly (exact
-// products) and folded into its (s, c) accumulator by TwoSum.  Each CTA
-// stores one compensated partial per row; k_struct_spmm_lfold adds them in
-// column-range order.
+// 16-bit entries).  One CTA of 1024 threads per (group, column range), two
+// shared-memory stages: a block's B rows (contiguous), row starts and records
+// arrive by bulk copies (completion on the stage's mbarrier, bounded waits).
+// Each warp walks the blocks on its own, multiplying out of shared memory:
+// LPN = N / 8 lanes per row, 8 columns (16 bytes) per lane, each row's
+// products of a block summed plainly (exact products) and folded into its
+// (s, c) accumulator by TwoSum.  A warp done with a block counts itself out
+// of the stage; the last one refills the stage with the block two ahead, so
+// no CTA-wide barrier separates blocks.  Each CTA stores one compensated
+// partial per row; k_struct_spmm_lfold adds them in column-range order.
 constexpr int kLtRows = 512;
 constexpr int kLtCols = 1024;
 constexpr int kLtRsEntries = 520;  // kLtRows + 1 starts, padded to 16 bytes
@@ -487,18 +488,15 @@ k_struct_spmm_ltile(const uint32_t* __restrict__ rec, const int64_t* __restrict_
     constexpr int kRsBytes = kLtRsEntries * 2;
     extern __shared__ __align__(128) unsigned char sm[];
     __shared__ __align__(8) uint64_t full[2];
+    __shared__ int done[2];    // warps finished with the block in each stage
+    __shared__ int issued_s;   // blocks whose copies were issued
+    constexpr int kWarps = kLtThreads / 32;
     const int stage_bytes = kBBytes + kRsBytes + rec_cap * 4;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int sub = lane / LPN, lig = lane % LPN;
     const int64_t g = blockIdx.x;
     const int64_t q = blockIdx.y, nq = gridDim.y;
     const int64_t j_lo = q * nbj / nq, j_hi = (q + 1) * nbj / nq;
-    if (tid == 0) {
-        tma::mbar_init(smem_u32(&full[0]), 1);
-        tma::mbar_init(smem_u32(&full[1]), 1);
-        tma::mbar_init_fence();
-    }
-    __syncthreads();
     auto issue = [&](int64_t j, int st) {
         const int64_t key = g * nbj + j;
         const int64_t rows_b = (n_cols - j * kLtCols) < kLtCols ? (n_cols - j * kLtCols) : kLtCols;
@@ -511,50 +509,66 @@ k_struct_spmm_ltile(const uint32_t* __restrict__ rec, const int64_t* __restrict_
         bulk_g2s(smem_u32(base + kBBytes), row_start + key * kLtRsEntries, kRsBytes, bar);
         if (r_bytes) bulk_g2s(smem_u32(base + kBBytes + kRsBytes), rec + seg_start[key], r_bytes, bar);
     };
+    if (tid == 0) {
+        tma::mbar_init(smem_u32(&full[0]), 1);
+        tma::mbar_init(smem_u32(&full[1]), 1);
+        tma::mbar_init_fence();
+        done[0] = done[1] = 0;
+        int n = 0;
+        if (j_lo < j_hi) issue(j_lo, 0), ++n;
+        if (j_lo + 1 < j_hi) issue(j_lo + 1, 1), ++n;
+        issued_s = n;
+    }
+    __syncthreads();
     comp_t acc[RPS][VW];
 #pragma unroll
     for (int i = 0; i < RPS; ++i)
 #pragma unroll
         for (int w = 0; w < VW; ++w) acc[i][w] = comp_t{0.f, 0.f};
     const int rig0 = (warp * NSUB + sub) * RPS;
-    if (tid == 0 && j_lo < j_hi) issue(j_lo, 0);
     bool ok = true;
-    int64_t j_fail = -1;
-    for (int64_t j = j_lo; j < j_hi && ok; ++j) {
+    // Each warp walks the blocks on its own: it waits for the block's copies,
+    // multiplies it, and releases the stage; the last warp to release a stage
+    // refills it with the block two ahead.  No CTA-wide barrier per block, so
+    // a warp with fewer records in a block runs ahead into the next one.
+    for (int64_t j = j_lo; j < j_hi; ++j) {
         const int st = (int)((j - j_lo) & 1);
         const uint32_t phase = (uint32_t)(((j - j_lo) >> 1) & 1);
-        // the other stage was released by every thread at the end of the last
-        // block: refill it with block j + 1 while this one is multiplied
-        if (tid == 0 && j + 1 < j_hi) issue(j + 1, st ^ 1);
-        ok = __syncthreads_and(mbar_wait(smem_u32(&full[st]), phase)) != 0;
-        if (!ok) {
-            j_fail = j;
-            break;
-        }
+        ok = __all_sync(0xffffffffu, mbar_wait(smem_u32(&full[st]), phase)) != 0;
+        if (!ok) break;
         const unsigned char* base = sm + (size_t)st * stage_bytes;
         const V* Bs = reinterpret_cast<const V*>(base);
         const uint16_t* rs = reinterpret_cast<const uint16_t*>(base + kBBytes);
         const uint32_t* rc = reinterpret_cast<const uint32_t*>(base + kBBytes + kRsBytes);
+        // one record: the B row slice as a single 16-byte shared load (the
+        // slice is 16-byte aligned: row * N * 2 + lig * 16 bytes), widened to
+        // float32 pairs, times the value, added by paired FMAs into blk (blk[h]
+        // holds columns 2h, 2h + 1 of the lane's slice)
+        uint64_t blk[VW / 2];
+        auto step = [&](uint32_t rr) {
+            const uint4 q4 = *reinterpret_cast<const uint4*>(Bs + (rr >> 16) * N + lig * VW);
+            const uint64_t a2 = lt_splat(lt_value<V>(rr & 0xffffu));
+            blk[0] = lt_fma2(a2, lt_widen2<V>(q4.x), blk[0]);
+            blk[1] = lt_fma2(a2, lt_widen2<V>(q4.y), blk[1]);
+            blk[2] = lt_fma2(a2, lt_widen2<V>(q4.z), blk[2]);
+            blk[3] = lt_fma2(a2, lt_widen2<V>(q4.w), blk[3]);
+        };
+        // a row's block sum (plain float32, exact products) enters its (s, c)
+        // accumulator by TwoSum
+        auto fold = [&](comp_t (&a)[VW]) {
+#pragma unroll
+            for (int h = 0; h < VW / 2; ++h) {
+                a[2 * h] = comp_add_value(a[2 * h], __uint_as_float((uint32_t)blk[h]), 0.f);
+                a[2 * h + 1] = comp_add_value(a[2 * h + 1], __uint_as_float((uint32_t)(blk[h] >> 32)), 0.f);
+                blk[h] = 0;
+            }
+        };
+#pragma unroll
+        for (int h = 0; h < VW / 2; ++h) blk[h] = 0;
 #pragma unroll
         for (int i = 0; i < RPS; ++i) {
             const int rig = rig0 + i;
             const int lo = rs[rig], hi = rs[rig + 1];
-            // the row's products of this block, summed plainly in float32
-            // pairs: blk[h] holds columns 2h, 2h + 1 of the lane's slice
-            uint64_t blk[VW / 2];
-#pragma unroll
-            for (int h = 0; h < VW / 2; ++h) blk[h] = 0;
-            // one record: the B row slice as a single 16-byte shared load (the
-            // slice is 16-byte aligned: row * N * 2 + lig * 16 bytes), widened
-            // to float32 pairs, times the value, added by paired FMAs
-            auto step = [&](uint32_t rr) {
-                const uint4 q4 = *reinterpret_cast<const uint4*>(Bs + (rr >> 16) * N + lig * VW);
-                const uint64_t a2 = lt_splat(lt_value<V>(rr & 0xffffu));
-                blk[0] = lt_fma2(a2, lt_widen2<V>(q4.x), blk[0]);
-                blk[1] = lt_fma2(a2, lt_widen2<V>(q4.y), blk[1]);
-                blk[2] = lt_fma2(a2, lt_widen2<V>(q4.z), blk[2]);
-                blk[3] = lt_fma2(a2, lt_widen2<V>(q4.w), blk[3]);
-            };
             int k = lo;
             for (; k + 1 < hi; k += 2) {  // two independent records in flight
                 const uint32_t r0 = rc[k], r1 = rc[k + 1];
@@ -562,24 +576,32 @@ k_struct_spmm_ltile(const uint32_t* __restrict__ rec, const int64_t* __restrict_
                 step(r1);
             }
             if (k < hi) step(rc[k]);
-            if (hi > lo) {
-#pragma unroll
-                for (int h = 0; h < VW / 2; ++h) {
-                    acc[i][2 * h] = comp_add_value(acc[i][2 * h], __uint_as_float((uint32_t)blk[h]), 0.f);
-                    acc[i][2 * h + 1] = comp_add_value(acc[i][2 * h + 1], __uint_as_float((uint32_t)(blk[h] >> 32)), 0.f);
+            if (hi > lo) fold(acc[i]);
+        }
+        // release the stage: the warp's shared-memory reads come before its
+        // arrival; the last warp to arrive refills the stage with block j + 2
+        __syncwarp();
+        if (lane == 0) {
+            __threadfence_block();
+            const int old = atomicAdd(&done[st], 1);
+            if (old == kWarps - 1) {
+                atomicExch(&done[st], 0);
+                __threadfence_block();
+                asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                if (j + 2 < j_hi) {
+                    issue(j + 2, st);
+                    atomicAdd(&issued_s, 1);
                 }
             }
         }
-        __syncthreads();  // stage st is free for block j + 2
     }
-    if (!ok) {
+    if (__syncthreads_or(!ok)) {
         if (tid == 0) {
             atomicExch(err, FSB_ERR_TIMEOUT);
-            // drain (bounded) the copies in flight before the CTA exits: block
-            // j_fail's and, when issued, block j_fail + 1's
-            const int64_t d = j_fail - j_lo;
-            mbar_wait(smem_u32(&full[d & 1]), (uint32_t)((d >> 1) & 1));
-            if (j_fail + 1 < j_hi) mbar_wait(smem_u32(&full[(d + 1) & 1]), (uint32_t)(((d + 1) >> 1) & 1));
+            // drain (bounded) every issued copy before the CTA exits: block
+            // j_lo + d completes phase (d >> 1) & 1 of stage d & 1
+            const int n = issued_s;
+            for (int d = (n > 2 ? n - 2 : 0); d < n; ++d) mbar_wait(smem_u32(&full[d & 1]), (uint32_t)((d >> 1) & 1));
         }
         return;
     }
