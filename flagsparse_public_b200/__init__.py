@@ -39,6 +39,10 @@ _EXPORTS = {
     "prepare_csr_mixed": "precision",
     "flagsparse_spmv_csr_mixed": "precision",
     "flagsparse_spmm_csr_mixed": "precision",
+    "benchmark_spmv_case": "benchmarks",
+    "benchmark_spmm_case": "benchmarks",
+    "benchmark_spmm_opt_case": "benchmarks",
+    "benchmark_spmm_opt_alg2_case": "benchmarks",
 }
 
 __all__ = sorted(_EXPORTS)

@@ -1,7 +1,8 @@
 """SpMV / SpMM operators with FlagSparse's ``sparse_operations`` interface.
 
 Re-exports the hot-path names of FlagSparse ``sparse_operations/__init__.py``
-(:29-54): CSR/COO SpMV, CSR SpMM (ALG1, opt, opt-alg2) and COO SpMM.
+(:29-54): CSR/COO SpMV, CSR SpMM (ALG1, opt, opt-alg2) and COO SpMM, and the
+benchmark entry points of that path.
 """
 
 from .spmv_csr import (
@@ -15,8 +16,18 @@ from .spmv_coo import PreparedCoo, flagsparse_spmv_coo, prepare_spmv_coo
 from .spmm_csr import PreparedCsrSpmmOpt, flagsparse_spmm_csr, flagsparse_spmm_csr_opt, prepare_spmm_csr_opt
 from .spmm_csr_opt_alg2 import PreparedCsrSpmmOptAlg2, flagsparse_spmm_csr_opt_alg2, prepare_spmm_csr_opt_alg2
 from .spmm_coo import flagsparse_spmm_coo
+from .benchmarks import (
+    benchmark_spmm_case,
+    benchmark_spmm_opt_alg2_case,
+    benchmark_spmm_opt_case,
+    benchmark_spmv_case,
+)
 
 __all__ = [
+    "benchmark_spmm_case",
+    "benchmark_spmm_opt_alg2_case",
+    "benchmark_spmm_opt_case",
+    "benchmark_spmv_case",
     "PreparedCoo",
     "PreparedCsrSpmv",
     "PreparedCsrSpmmOpt",
