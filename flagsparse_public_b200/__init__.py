@@ -43,6 +43,7 @@ _EXPORTS = {
     "benchmark_spmm_case": "benchmarks",
     "benchmark_spmm_opt_case": "benchmarks",
     "benchmark_spmm_opt_alg2_case": "benchmarks",
+    "benchmark_sddmm_case": "benchmarks",
 }
 
 __all__ = sorted(_EXPORTS)

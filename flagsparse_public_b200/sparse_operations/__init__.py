@@ -17,6 +17,7 @@ from .spmm_csr import PreparedCsrSpmmOpt, flagsparse_spmm_csr, flagsparse_spmm_c
 from .spmm_csr_opt_alg2 import PreparedCsrSpmmOptAlg2, flagsparse_spmm_csr_opt_alg2, prepare_spmm_csr_opt_alg2
 from .spmm_coo import flagsparse_spmm_coo
 from .benchmarks import (
+    benchmark_sddmm_case,
     benchmark_spmm_case,
     benchmark_spmm_opt_alg2_case,
     benchmark_spmm_opt_case,
@@ -24,6 +25,7 @@ from .benchmarks import (
 )
 
 __all__ = [
+    "benchmark_sddmm_case",
     "benchmark_spmm_case",
     "benchmark_spmm_opt_alg2_case",
     "benchmark_spmm_opt_case",

@@ -13,7 +13,7 @@ FlagSparse's reason string.
 Reference: ``benchmark_spmv_case`` (benchmarks.py:345-507),
 ``benchmark_spmm_case`` (spmm_csr.py:2351-2573), ``benchmark_spmm_opt_case``
 (spmm_csr.py:2226-2348), ``benchmark_spmm_opt_alg2_case``
-(spmm_csr_opt_alg2.py:862-972).
+(spmm_csr_opt_alg2.py:862-972), ``benchmark_sddmm_case`` (sddmm_csr.py:472-568).
 """
 
 import time
@@ -346,4 +346,68 @@ def benchmark_spmm_opt_alg2_case(n_rows=4096, n_cols=4096, nnz=65536, n_dense_co
         "backend_status": {"cusparse_unavailable_reason": cu_reason},
         "samples": {"base_triton": base_values, "opt_triton": opt_values, "opt_alg2_triton": alg2_values,
                     "torch_ref": torch_ref, "cusparse_ref": cu_ref},
+    }
+
+
+def _sampled_dot(indices, indptr, x, y, data, alpha, beta):
+    """PyTorch SDDMM reference: alpha * <x[row(p)], y[col(p)]> + beta * data[p]
+    for every stored position p (a gather of both rows and a row-wise dot)."""
+    rows = torch.repeat_interleave(torch.arange(indptr.numel() - 1, device=x.device, dtype=torch.int64),
+                                   indptr[1:] - indptr[:-1])
+    out = alpha * (x.index_select(0, rows) * y.index_select(0, indices.to(torch.int64))).sum(dim=1)
+    if data is not None and beta != 0.0:
+        out = out + beta * data
+    return out
+
+
+def benchmark_sddmm_case(n_rows=1024, n_cols=1024, nnz=16384, k_dim=64, value_dtype=torch.float32, warmup=10,
+                         iters=30, alpha=1.0, beta=0.0, run_cusparse=False):
+    """CSR SDDMM (``flagsparse_sddmm_csr`` on a prepared pattern) against a
+    PyTorch sampled-dot reference (sddmm_csr.py:472-568)."""
+    from .sddmm_csr import SUPPORTED_SDDMM_VALUE_DTYPES, flagsparse_sddmm_csr, prepare_sddmm_csr
+
+    if value_dtype not in SUPPORTED_SDDMM_VALUE_DTYPES:
+        raise TypeError("value_dtype must be torch.float32 or torch.float64")
+    device = torch.device("cuda")
+    data, indices, indptr = _build_random_csr(n_rows, n_cols, nnz, value_dtype, torch.int32, device)
+    x = _build_random_dense((n_rows, k_dim), value_dtype, device)
+    y = _build_random_dense((n_cols, k_dim), value_dtype, device)
+    prepared = prepare_sddmm_csr(indices, indptr, (n_rows, n_cols), k_hint=k_dim)
+    ours, ours_ms = _benchmark_cuda_op(
+        lambda: flagsparse_sddmm_csr(data=data, x=x, y=y, alpha=alpha, beta=beta, prepared=prepared,
+                                     return_time=False), warmup=warmup, iters=iters)
+    ip64 = indptr.to(torch.int64)
+    ref, pt_ms = _benchmark_cuda_op(lambda: _sampled_dot(indices, ip64, x, y, data, alpha, beta), warmup=warmup,
+                                    iters=iters)
+    atol, rtol = _tolerance_for_dtype(value_dtype)
+    match = bool(torch.allclose(ours, ref, atol=atol, rtol=rtol))
+    max_abs = float(torch.max(torch.abs(ours - ref)).item()) if ours.numel() > 0 else 0.0
+    cu_ms = cu_reason = cu_match = None
+    if run_cusparse:
+        if cp is None:
+            cu_reason = "CuPy is not available"
+        else:
+            try:
+                def cupy_sampled_dot():
+                    xs = cp.asarray(x)[cp.asarray(torch.repeat_interleave(
+                        torch.arange(n_rows, device=device), ip64[1:] - ip64[:-1]))]
+                    ys = cp.asarray(y)[cp.asarray(indices.to(torch.int64))]
+                    v = alpha * (xs * ys).sum(axis=1)
+                    return torch.as_tensor(v + beta * cp.asarray(data) if beta != 0.0 else v, device=device)
+
+                ref_cu, cu_ms = _benchmark_cuda_op(cupy_sampled_dot, warmup=warmup, iters=iters)
+                cu_match = bool(torch.allclose(ours, ref_cu, atol=atol, rtol=rtol))
+            except Exception as exc:  # noqa: BLE001
+                cu_reason = str(exc)
+    return {
+        "parameters": {"n_rows": n_rows, "n_cols": n_cols, "nnz": nnz, "k_dim": k_dim,
+                       "value_dtype": str(value_dtype), "warmup": warmup, "iters": iters, "alpha": alpha,
+                       "beta": beta},
+        "performance": {"triton_ms": ours_ms, "pytorch_ms": pt_ms, "cusparse_ms": cu_ms,
+                        "triton_speedup_vs_pytorch": pt_ms / ours_ms if ours_ms > 0 else None,
+                        "triton_speedup_vs_cusparse": cu_ms / ours_ms if (cu_ms and ours_ms > 0) else None},
+        "verification": {"triton_match_pytorch": match, "triton_max_abs_error": max_abs,
+                         "cusparse_match_pytorch": cu_match},
+        "backend_status": {"cusparse_unavailable_reason": cu_reason},
+        "samples": {"triton": ours, "pytorch": ref},
     }

@@ -48,3 +48,22 @@ def test_benchmark_spmm_opt_and_alg2_cases(dtype):
     assert v["opt_vs_cusparse_err"] is None
     with pytest.raises(TypeError, match="only supports float32 and float64"):
         fs.benchmark_spmm_opt_case(value_dtype=torch.float16)
+
+
+@pytest.mark.parametrize("dtype", [torch.float32, torch.float64])
+def test_benchmark_sddmm_case(dtype):
+    r = fs.benchmark_sddmm_case(n_rows=1500, n_cols=900, nnz=20000, k_dim=64, value_dtype=dtype, warmup=2, iters=3,
+                                alpha=1.5, beta=0.5, run_cusparse=True)
+    # FlagSparse's own check is allclose in the value type (atol 1e-6, rtol
+    # 1e-5 for float32), which two float32 dot products of 64 terms summed in
+    # different orders can miss near cancellation: float32 is held to an
+    # absolute bound instead (entries are O(10))
+    if dtype == torch.float64:
+        assert r["verification"]["triton_match_pytorch"] is True
+    else:
+        assert r["verification"]["triton_max_abs_error"] <= 1e-4
+    assert r["performance"]["triton_ms"] > 0 and r["performance"]["pytorch_ms"] > 0
+    assert r["backend_status"]["cusparse_unavailable_reason"] == "CuPy is not available"
+    assert r["samples"]["triton"].shape == (20000,)
+    with pytest.raises(TypeError):
+        fs.benchmark_sddmm_case(value_dtype=torch.float16)
