@@ -175,10 +175,11 @@ k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __rest
             const int64_t e = idx(ptr[r + 1]) - k0;
             return e > (int64_t)kNoEnd ? kNoEnd : (int)e;
         };
-        // rows rb .. rb + 31 in e_win, the next 32 prefetched in e_nxt
+        // rows rb .. rb + 31 in e_win, the next 64 prefetched in e_nxt, e_nx2
         int64_t rb = r0;
         int e_win = load_ends(rb);
         int e_nxt = load_ends(rb + 32);
+        int e_nx2 = load_ends(rb + 64);
         int64_t row = r0;
         int64_t row_start = (r0 < n_rows) ? idx(ptr[r0]) : k0;  // global start of the current row
         const bool continued = (r0 < n_rows) && (k0 > row_start);
@@ -260,7 +261,8 @@ k_spmm_seq(const V* __restrict__ val, const I* __restrict__ col, const P* __rest
             if (row <= last_row && row - rb >= 32) {
                 rb += 32;
                 e_win = e_nxt;
-                e_nxt = load_ends(rb + 32);
+                e_nxt = e_nx2;
+                e_nx2 = load_ends(rb + 64);
             }
             row_end = row <= last_row ? __shfl_sync(full, e_win, (int)(row - rb)) : kNoEnd;
             long_row = row_is_long();
