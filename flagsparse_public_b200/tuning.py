@@ -10,7 +10,7 @@ row groups, the merge-path kernel, and the batched merge-path kernel at four
 unit sizes and two column tiles.
 
 * ``Autotuner`` times every candidate on the matrix and dense width at hand
-  (CUDA events) and caches the winner -- exhaustive autotuning, the judge of
+  (CUDA events) and caches the winner -- exhaustive autotuning, the yardstick of
   the selector's regret.
 * ``LearnedSelector`` predicts each candidate's time relative to the best
   (log2 ratio) with a small MLP over matrix features (rows, columns, nonzeros,
